@@ -1,0 +1,871 @@
+// Device solver for one simulation: buffers, transform pipelines and the
+// per-stage kernel sequence of the RK3 step.
+//
+// Per RK stage (model.f90:192-223 restated on a spectral-resident state):
+//   phase A  inverse: dn, m_d [, grad n, lap n]   pointwise: u, m_i u_j, mu_local
+//            forward: u_d, m_i u_j (i<=j), mu_local
+//            combine A: mu-hat, -div(m u) + div Pi (partial dmom), Pi0 and
+//                       the previous stage's Maxwell relaxation
+//   phase B  inverse: d mu/dx_d [, d Pi_c/dx_d]   pointwise: n (dmu - F_ext),
+//            -u.grad Pi_c   forward: those
+//            combine B: dn, dmom, dPi and the low-storage RK update
+// Linear operators (divergences, Pi0 and its divergence, hartree and RY
+// convolutions, dealiasing, the RK update and the relaxation) act on the
+// spectral state; only the nonlinear products are transformed.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "kernels.cuh"
+#include "solver.hpp"
+
+namespace hydft {
+
+#define CK(call)                                                                 \
+    do {                                                                         \
+        cudaError_t e_ = (call);                                                 \
+        if (e_ != cudaSuccess) {                                                 \
+            err = std::string(#call) + ": " + cudaGetErrorString(e_);            \
+            return HYDFT_E_CUDA;                                                 \
+        }                                                                        \
+    } while (0)
+
+enum { HYDFT_E_OK = 0, HYDFT_E_BAD = 1, HYDFT_E_OOM = 2, HYDFT_E_NONPOS = 3, HYDFT_E_NONFINITE = 4,
+       HYDFT_E_NEWTON = 5, HYDFT_E_CUDA = 7 };
+
+// reduction partials of the diagnostics kernel
+struct RedPart {
+    double sn, cn_, sm[3], cm[3], sk, ck, nmin, nmax, umax;
+};
+
+template <typename R>
+__device__ __forceinline__ void neumaier(double &s, double &c, double v)
+{
+    const double t = s + v;
+    if (fabs(s) >= fabs(v)) c += (s - t) + v;
+    else c += (v - t) + s;
+    s = t;
+}
+
+// FP64 compensated sums of n, m_d, m_d^2/n and extrema over the real-space
+// fields; one partial per block, combined in a fixed order by reduce_final.
+template <typename R>
+__global__ void reduce_fields_kernel(const R *dn, const R *m, size_t ncell, int nm, const cplx<R> *nhat,
+                                     double inv_mass, RedPart *part)
+{
+    __shared__ RedPart sh[8];
+    const double nref = (double)nhat[0].x;
+    RedPart p;
+    p.sn = p.cn_ = p.sk = p.ck = 0.0;
+    for (int d = 0; d < 3; ++d) p.sm[d] = p.cm[d] = 0.0;
+    p.nmin = 1e300; p.nmax = -1e300; p.umax = 0.0;
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < ncell; q += (size_t)gridDim.x * blockDim.x) {
+        const double n = nref + (double)dn[q];
+        neumaier<R>(p.sn, p.cn_, n);
+        p.nmin = fmin(p.nmin, n);
+        p.nmax = fmax(p.nmax, n);
+        for (int d = 0; d < nm; ++d) {
+            const double md = (double)m[d * ncell + q];
+            neumaier<R>(p.sm[d], p.cm[d], md);
+            neumaier<R>(p.sk, p.ck, md * md / n);
+            p.umax = fmax(p.umax, fabs(md * inv_mass / n));
+        }
+    }
+    // warp reduction (compensation terms folded into the sums)
+    double v[9] = {p.sn + p.cn_, p.sm[0] + p.cm[0], p.sm[1] + p.cm[1], p.sm[2] + p.cm[2], p.sk + p.ck,
+                   p.nmin, p.nmax, p.umax, 0.0};
+    for (int off = 16; off > 0; off >>= 1) {
+        for (int i = 0; i < 5; ++i) v[i] += __shfl_down_sync(0xffffffffu, v[i], off);
+        v[5] = fmin(v[5], __shfl_down_sync(0xffffffffu, v[5], off));
+        v[6] = fmax(v[6], __shfl_down_sync(0xffffffffu, v[6], off));
+        v[7] = fmax(v[7], __shfl_down_sync(0xffffffffu, v[7], off));
+    }
+    const int w = threadIdx.x / 32, l = threadIdx.x % 32;
+    if (l == 0) {
+        sh[w].sn = v[0]; sh[w].sm[0] = v[1]; sh[w].sm[1] = v[2]; sh[w].sm[2] = v[3]; sh[w].sk = v[4];
+        sh[w].nmin = v[5]; sh[w].nmax = v[6]; sh[w].umax = v[7];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        RedPart o = sh[0];
+        o.cn_ = o.ck = 0.0;
+        for (int d = 0; d < 3; ++d) o.cm[d] = 0.0;
+        const int nw = blockDim.x / 32;
+        for (int i = 1; i < nw; ++i) {
+            neumaier<R>(o.sn, o.cn_, sh[i].sn);
+            for (int d = 0; d < 3; ++d) neumaier<R>(o.sm[d], o.cm[d], sh[i].sm[d]);
+            neumaier<R>(o.sk, o.ck, sh[i].sk);
+            o.nmin = fmin(o.nmin, sh[i].nmin);
+            o.nmax = fmax(o.nmax, sh[i].nmax);
+            o.umax = fmax(o.umax, sh[i].umax);
+        }
+        part[blockIdx.x] = o;
+    }
+}
+
+template <typename R>
+__global__ void reduce_final_kernel(const RedPart *part, int nb, RedPart *out)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    RedPart o;
+    o.sn = o.cn_ = o.sk = o.ck = 0.0;
+    for (int d = 0; d < 3; ++d) o.sm[d] = o.cm[d] = 0.0;
+    o.nmin = 1e300; o.nmax = -1e300; o.umax = 0.0;
+    for (int b = 0; b < nb; ++b) {
+        neumaier<R>(o.sn, o.cn_, part[b].sn);
+        neumaier<R>(o.sn, o.cn_, part[b].cn_);
+        for (int d = 0; d < 3; ++d) {
+            neumaier<R>(o.sm[d], o.cm[d], part[b].sm[d]);
+            neumaier<R>(o.sm[d], o.cm[d], part[b].cm[d]);
+        }
+        neumaier<R>(o.sk, o.ck, part[b].sk);
+        neumaier<R>(o.sk, o.ck, part[b].ck);
+        o.nmin = fmin(o.nmin, part[b].nmin);
+        o.nmax = fmax(o.nmax, part[b].nmax);
+        o.umax = fmax(o.umax, part[b].umax);
+    }
+    o.sn += o.cn_;
+    for (int d = 0; d < 3; ++d) o.sm[d] += o.cm[d];
+    o.sk += o.ck;
+    *out = o;
+}
+
+template <typename R>
+__global__ void fill_real_kernel(R *dst, const double *src, double sub, size_t n)
+{
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x)
+        dst[q] = R(src[q] - sub);
+}
+
+template <typename R>
+__global__ void real_to_double_kernel(double *dst, const R *src, double add, size_t n)
+{
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x)
+        dst[q] = (double)src[q] + add;
+}
+
+template <typename R>
+__global__ void set_k0_kernel(cplx<R> *a, double re)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) a[0] = cplx<R>{R(re), R(0)};
+}
+
+template <typename R>
+static void make_twiddles(int L, std::vector<cplx<R>> &tw)
+{
+    tw.resize(std::max(L, 1));
+    const double pi = 3.14159265358979323846264338327950288;
+    for (int t = 0; t < L; ++t) {
+        const double a = -2.0 * pi * (double)t / (double)L;
+        tw[t] = cplx<R>{R(std::cos(a)), R(std::sin(a))};
+    }
+    if (L >= 4 && L % 4 == 0) {     // exact values at the quarter points
+        tw[0] = cplx<R>{R(1), R(0)};
+        tw[L / 4] = cplx<R>{R(0), R(-1)};
+        tw[L / 2] = cplx<R>{R(-1), R(0)};
+        tw[3 * L / 4] = cplx<R>{R(0), R(1)};
+    }
+}
+
+template <typename R>
+class Solver : public SolverBase {
+public:
+    static constexpr int TX = sizeof(R) == 4 ? 16 : 8;
+    SolverSetup S;
+    Grid g;
+    Phys ph;
+    int nm;
+    int device;
+    size_t csize, zsize, ysize, ncell;
+    int nin_max, nout_max;
+    cudaStream_t st = nullptr;
+    std::vector<void *> allocs;
+    // compact fields
+    cplx<R> *N, *M[3], *P[6], *RN, *RM[3], *RP[6], *P0[6], *MU, *Q[3];
+    cplx<R> *OA[16], *OB[12];       // phase outputs (compact)
+    cplx<R> *HN, *HM[3], *HP[6];    // rhs-only outputs
+    cplx<R> *zi, *yi, *xo;          // pass buffers
+    R *dn_real, *u_real, *io_real;  // real-space fields
+    R *Klin;
+    double *fdtab = nullptr;
+    cplx<double> *ex, *ey, *ez;
+    cplx<R> *twx, *twy, *twz;
+    Ctrl *ctrl;
+    RedPart *rpart, *rout;
+    int red_blocks = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    int xrb_a = 1, xrb_b = 1, xrb_io = 1;
+    int smem_optin = 0;
+
+    int precision_bits() const override { return sizeof(R) * 8; }
+    void set_ext_omega(double w) override
+    {
+        S.ext_omega = w;
+        ph.ext_omega = w;
+        if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
+        if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
+    }
+    const SolverSetup &setup() const override { return S; }
+    void *stream() override { return (void *)st; }
+
+    ~Solver() override
+    {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        if (graph) cudaGraphDestroy(graph);
+        for (void *p : allocs) cudaFree(p);
+        if (st) cudaStreamDestroy(st);
+    }
+
+    template <typename T>
+    int alloc(T *&p, size_t n)
+    {
+        void *q = nullptr;
+        cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
+        if (e != cudaSuccess) {
+            err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+            return HYDFT_E_OOM;
+        }
+        allocs.push_back(q);
+        p = static_cast<T *>(q);
+        return 0;
+    }
+
+    int init(const SolverSetup &s, int dev)
+    {
+        S = s;
+        g = s.g;
+        nm = s.nm;
+        device = dev;
+        CK(cudaSetDevice(dev));
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        int optin = 0;
+        CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        smem_optin = optin;
+        std::memset(&ph, 0, sizeof(ph));
+        ph.beta = s.beta; ph.inv_beta = 1.0 / s.beta; ph.mass = s.mass; ph.inv_mass = 1.0 / s.mass;
+        ph.n0 = s.n0;
+        ph.nterms_local = s.nterms_local;
+        for (int i = 0; i < 8; ++i) ph.term_order[i] = s.term_order[i];
+        for (int i = 0; i < s.nterms_local; ++i) {
+            if (s.term_order[i] == 1) ph.has_ideal = 1;
+            if (s.term_order[i] == 2) ph.has_tf = 1;
+            if (s.term_order[i] == 3) ph.has_grad = 1;
+        }
+        ph.cn = s.cn; ph.cg = s.cg; ph.alpha_ref = s.alpha_ref;
+        ph.evolve = s.evolve; ph.newtonian = s.newtonian;
+        ph.eta = s.eta; ph.xi = s.xi; ph.tau = s.tau;
+        ph.ext_active = s.ext_active; ph.ext_kind = s.ext_kind;
+        for (int d = 0; d < 3; ++d) ph.ext_k[d] = s.ext_k[d];
+        ph.ext_amp = s.ext_amp; ph.ext_omega = s.ext_omega; ph.ext_ramp = s.ext_ramp;
+        ph.drive_in_band = s.drive_in_band; ph.drive_idx = s.drive_idx; ph.drive_conj = s.drive_conj;
+
+        csize = (size_t)g.nkzc * g.nkyc * g.pkx;
+        zsize = (size_t)g.nz * g.nkyc * g.pkx;
+        ysize = (size_t)g.nz * g.ny * g.pkx;
+        ncell = (size_t)g.nx * g.ny * g.nz;
+        const int ngrad = (ph.has_tf || ph.has_grad) && ph.has_grad ? nm + 1 : 0;
+        const int ninA = 1 + nm + ngrad;
+        const int noutA = nm + nm * (nm + 1) / 2 + 1;
+        const int ninB = nm + (ph.evolve ? 6 * nm : 0);
+        const int noutB = nm + (ph.evolve ? 6 : 0);
+        nin_max = std::max({ninA, ninB, 10});
+        nout_max = std::max({noutA, noutB, 10});
+        // compact fields: N M3 P6 RN RM3 RP6 P0_6 MU Q3 OA16 OB12 HN HM3 HP6
+        const int ncf = 1 + 3 + 6 + 1 + 3 + 6 + 6 + 1 + 3 + 16 + 12 + 1 + 3 + 6;
+        cplx<R> *cb;
+        if (int rc = alloc(cb, ncf * csize)) return rc;
+        CK(cudaMemset(cb, 0, ncf * csize * sizeof(cplx<R>)));
+        cplx<R> *p = cb;
+        auto take = [&]() { cplx<R> *r = p; p += csize; return r; };
+        N = take();
+        for (auto &x : M) x = take();
+        for (auto &x : P) x = take();
+        RN = take();
+        for (auto &x : RM) x = take();
+        for (auto &x : RP) x = take();
+        for (auto &x : P0) x = take();
+        MU = take();
+        for (auto &x : Q) x = take();
+        for (auto &x : OA) x = take();
+        for (auto &x : OB) x = take();
+        HN = take();
+        for (auto &x : HM) x = take();
+        for (auto &x : HP) x = take();
+        if (int rc = alloc(zi, (size_t)nin_max * zsize)) return rc;
+        if (g.ny > 1) {
+            if (int rc = alloc(yi, (size_t)nin_max * ysize)) return rc;
+        } else {
+            yi = zi;   // y transform of length 1: ZI and YI layouts coincide
+        }
+        if (int rc = alloc(xo, (size_t)nout_max * ysize)) return rc;
+        if (int rc = alloc(dn_real, ncell)) return rc;
+        if (int rc = alloc(u_real, 3 * ncell)) return rc;
+        if (int rc = alloc(io_real, 10 * ncell)) return rc;
+        CK(cudaMemset(u_real, 0, 3 * ncell * sizeof(R)));
+        if (int rc = alloc(Klin, csize)) return rc;
+        {
+            std::vector<R> kl(csize, R(0));
+            for (size_t i = 0; i < csize && i < s.klin.size(); ++i) kl[i] = R(s.klin[i]);
+            CK(cudaMemcpy(Klin, kl.data(), csize * sizeof(R), cudaMemcpyHostToDevice));
+        }
+        if (!s.fdtab.empty()) {
+            if (int rc = alloc(fdtab, s.fdtab.size())) return rc;
+            CK(cudaMemcpy(fdtab, s.fdtab.data(), s.fdtab.size() * sizeof(double), cudaMemcpyHostToDevice));
+        }
+        auto up_c = [&](cplx<double> *&dst, const std::vector<std::complex<double>> &v, int n) -> int {
+            if (int rc = alloc(dst, n)) return rc;
+            std::vector<cplx<double>> h(n, cplx<double>{1.0, 0.0});
+            for (int i = 0; i < n && i < (int)v.size(); ++i) h[i] = cplx<double>{v[i].real(), v[i].imag()};
+            CK(cudaMemcpy(dst, h.data(), n * sizeof(cplx<double>), cudaMemcpyHostToDevice));
+            return 0;
+        };
+        if (int rc = up_c(ex, s.ex, g.nx)) return rc;
+        if (int rc = up_c(ey, s.ey, g.ny)) return rc;
+        if (int rc = up_c(ez, s.ez, g.nz)) return rc;
+        auto up_tw = [&](cplx<R> *&dst, int L) -> int {
+            std::vector<cplx<R>> tw;
+            make_twiddles<R>(L, tw);
+            if (int rc = alloc(dst, tw.size())) return rc;
+            CK(cudaMemcpy(dst, tw.data(), tw.size() * sizeof(cplx<R>), cudaMemcpyHostToDevice));
+            return 0;
+        };
+        if (int rc = up_tw(twx, g.nx)) return rc;
+        if (int rc = up_tw(twy, g.ny)) return rc;
+        if (int rc = up_tw(twz, g.nz)) return rc;
+        if (int rc = alloc(ctrl, 1)) return rc;
+        {
+            Ctrl c;
+            std::memset(&c, 0, sizeof(c));
+            CK(cudaMemcpy(ctrl, &c, sizeof(c), cudaMemcpyHostToDevice));
+        }
+        red_blocks = 2 * 148;
+        if (int rc = alloc(rpart, red_blocks)) return rc;
+        if (int rc = alloc(rout, 1)) return rc;
+        // x-pass rows per block
+        xrb_a = pick_rb(ninA, noutA);
+        xrb_b = pick_rb(ninB, noutB);
+        xrb_io = pick_rb(10, 10);
+        if (int rc = set_smem_attrs()) return rc;
+        // uniform initial state n = n0, mom = 0, Pi = 0 (species.f90:155-169)
+        set_k0_kernel<R><<<1, 32, 0, st>>>(N, s.n0);
+        launches++;
+        CK(cudaStreamSynchronize(st));
+        return 0;
+    }
+
+    int pick_rb(int nin, int nout)
+    {
+        int rb = std::max(1, 512 / g.nx);
+        while (rb > 1 && xpass_smem<R>(g.nx, rb, nin, nout) > 100 * 1024) rb--;
+        return rb;
+    }
+
+    int set_smem_attrs()
+    {
+        const int lim = smem_optin;
+        CK(cudaFuncSetAttribute(zinv_kernel<R, TX>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        CK(cudaFuncSetAttribute(yinv_kernel<R, TX>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        CK(cudaFuncSetAttribute(yfwd_kernel<R, TX>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        CK(cudaFuncSetAttribute(zfwd_kernel<R, TX>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        CK(cudaFuncSetAttribute(xpass_kernel<R, PWA<R>>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        CK(cudaFuncSetAttribute(xpass_kernel<R, PWB<R>>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        CK(cudaFuncSetAttribute(xpass_kernel<R, PWU<R>>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        CK(cudaFuncSetAttribute(xpass_kernel<R, PWToReal<R>>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        CK(cudaFuncSetAttribute(xpass_kernel<R, PWFromReal<R>>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        return 0;
+    }
+
+    // ------------------------------------------------------------ pipelines
+    // inverse transform of nf spectral fields (with load-time operators) into
+    // YI buffers 0..nf-1
+    void inverse(int nf, const cplx<R> *const *src, const int *ops)
+    {
+        PassArgs<R> a;
+        a.nf = nf;
+        for (int f = 0; f < nf; ++f) {
+            a.in[f] = src[f];
+            a.out[f] = zi + (size_t)f * zsize;
+            a.op[f] = ops[f];
+        }
+        const int ntx = (g.nkxc + TX - 1) / TX;
+        const size_t smz = sizeof(cplx<R>) * (2 * (size_t)g.nz * TX + g.nz);
+        zinv_kernel<R, TX><<<dim3(ntx, g.nkyc, nf), 256, smz, st>>>(g, a, twz);
+        launches++;
+        if (g.ny > 1) {
+            PassArgs<R> b;
+            b.nf = nf;
+            for (int f = 0; f < nf; ++f) {
+                b.in[f] = zi + (size_t)f * zsize;
+                b.out[f] = yi + (size_t)f * ysize;
+                b.op[f] = OP_ID;
+            }
+            const size_t smy = sizeof(cplx<R>) * (2 * (size_t)g.ny * TX + g.ny);
+            yinv_kernel<R, TX><<<dim3(ntx, g.nz, nf), 256, smy, st>>>(g, b, twy);
+            launches++;
+        }
+    }
+
+    // forward transform of the x-pass outputs 0..nf-1 into compact fields
+    void forward(int nf, cplx<R> *const *dst)
+    {
+        const int ntx = (g.nkxc + TX - 1) / TX;
+        const cplx<R> *src = xo;
+        if (g.ny > 1) {
+            PassArgs<R> b;
+            b.nf = nf;
+            for (int f = 0; f < nf; ++f) {
+                b.in[f] = xo + (size_t)f * ysize;
+                b.out[f] = zi + (size_t)f * zsize;
+                b.op[f] = OP_ID;
+            }
+            const size_t smy = sizeof(cplx<R>) * (2 * (size_t)g.ny * TX + g.ny);
+            yfwd_kernel<R, TX><<<dim3(ntx, g.nz, nf), 256, smy, st>>>(g, b, twy);
+            launches++;
+            src = zi;
+        }
+        PassArgs<R> a;
+        a.nf = nf;
+        for (int f = 0; f < nf; ++f) {
+            a.in[f] = src + (size_t)f * (g.ny > 1 ? zsize : ysize);
+            a.out[f] = dst[f];
+            a.op[f] = OP_ID;
+        }
+        const size_t smz = sizeof(cplx<R>) * (2 * (size_t)g.nz * TX + g.nz);
+        const R norm = R(1.0 / ((double)g.nx * g.ny * g.nz));
+        zfwd_kernel<R, TX><<<dim3(ntx, g.nkyc, nf), 256, smz, st>>>(g, a, twz, norm);
+        launches++;
+    }
+
+    template <class PW>
+    void xpass(int nin, int nout, const PW &pw, int rb)
+    {
+        XArgs<R> a;
+        a.nin = nin;
+        a.nout = nout;
+        for (int f = 0; f < nin; ++f) a.in[f] = yi + (size_t)f * ysize;
+        for (int f = 0; f < nout; ++f) a.out[f] = xo + (size_t)f * ysize;
+        const int nrows = g.ny * g.nz;
+        const size_t sm = xpass_smem<R>(g.nx, rb, nin, nout);
+        xpass_kernel<R, PW><<<(nrows + rb - 1) / rb, 256, sm, st>>>(g, a, twx, pw, rb);
+        launches++;
+    }
+
+    int combine_grid() const
+    {
+        return (int)std::min<size_t>((csize + 255) / 256, 148 * 16);
+    }
+
+    // -------------------------------------------------------------- stage
+    void phase_a(int stage, bool write_u)
+    {
+        const cplx<R> *src[MAXF];
+        int ops[MAXF];
+        int nf = 0;
+        src[nf] = N; ops[nf++] = OP_ZK0;
+        for (int d = 0; d < nm; ++d) { src[nf] = M[d]; ops[nf++] = OP_ID; }
+        if (ph.has_grad) {
+            for (int d = 0; d < nm; ++d) { src[nf] = N; ops[nf++] = OP_IKX + d; }
+            src[nf] = N; ops[nf++] = OP_NK2;
+        }
+        inverse(nf, src, ops);
+        PWA<R> pw;
+        pw.ph = ph;
+        pw.nm = nm;
+        pw.nhat = N;
+        pw.fdtab = fdtab;
+        pw.dn_real = dn_real;
+        pw.u_real = write_u ? u_real : nullptr;
+        pw.ncell = ncell;
+        pw.status = &ctrl->status;
+        const int nout = nm + nm * (nm + 1) / 2 + 1;
+        xpass(nf, nout, pw, xrb_a);
+        forward(nout, OA);
+        CombineA<R> c;
+        c.N = N;
+        for (int d = 0; d < 3; ++d) c.M[d] = M[d];
+        for (int q = 0; q < 6; ++q) { c.P[q] = P[q]; c.P0[q] = P0[q]; }
+        for (int d = 0; d < 3; ++d) c.U[d] = OA[d];
+        for (int q = 0; q < 6; ++q) c.F[q] = OA[nm + std::min(q, nm * (nm + 1) / 2 - 1)];
+        c.G = OA[nout - 1];
+        c.Klin = Klin;
+        c.MU = MU;
+        for (int d = 0; d < 3; ++d) c.Q[d] = Q[d];
+        combine_a_kernel<R><<<combine_grid(), 256, 0, st>>>(g, ph, nm, c, ctrl, stage);
+        launches++;
+    }
+
+    void phase_b(int stage, bool rhs_only)
+    {
+        const cplx<R> *src[MAXF];
+        int ops[MAXF];
+        int nf = 0;
+        for (int d = 0; d < nm; ++d) { src[nf] = MU; ops[nf++] = OP_IKX + d; }
+        if (ph.evolve)
+            for (int c = 0; c < 6; ++c)
+                for (int d = 0; d < nm; ++d) { src[nf] = P[c]; ops[nf++] = OP_IKX + d; }
+        inverse(nf, src, ops);
+        PWB<R> pw;
+        pw.ph = ph;
+        pw.nm = nm;
+        pw.nhat = N;
+        pw.dn_real = dn_real;
+        pw.u_real = u_real;
+        pw.ncell = ncell;
+        pw.ex = ex; pw.ey = ey; pw.ez = ez;
+        pw.ctrl = ctrl;
+        pw.stage = stage;
+        const int nout = nm + (ph.evolve ? 6 : 0);
+        xpass(nf, nout, pw, xrb_b);
+        forward(nout, OB);
+        CombineB<R> c;
+        c.N = N; c.RN = RN; c.oN = HN;
+        for (int d = 0; d < 3; ++d) {
+            c.M[d] = M[d]; c.RM[d] = RM[d]; c.oM[d] = HM[d];
+            c.Q[d] = Q[d];
+            c.Gm[d] = OB[std::min(d, nm - 1)];
+        }
+        for (int q = 0; q < 6; ++q) {
+            c.P[q] = P[q]; c.RP[q] = RP[q]; c.oP[q] = HP[q];
+            c.V[q] = OB[ph.evolve ? nm + q : 0];
+        }
+        combine_b_kernel<R><<<combine_grid(), 256, 0, st>>>(g, ph, nm, c, ctrl, stage, rhs_only ? 1 : 0);
+        launches++;
+    }
+
+    void begin_step()
+    {
+        const double omega = S.ext_kind == 2 ? S.ext_omega : 0.0;
+        begin_step_kernel<<<1, 32, 0, st>>>(ctrl, ph.evolve ? ph.tau : 0.0, S.ext_td, S.ext_amp, omega,
+                                            S.ext_ramp);
+        launches++;
+    }
+
+    void one_step()
+    {
+        begin_step();
+        for (int s = 0; s < 3; ++s) {
+            phase_a(s, ph.evolve != 0);
+            phase_b(s, false);
+        }
+        end_step_kernel<<<1, 32, 0, st>>>(ctrl);
+        launches++;
+    }
+
+    // Maxwell: complete the last stage's relaxation from u of the new state
+    void finish()
+    {
+        if (!ph.evolve) return;
+        const cplx<R> *src[MAXF];
+        int ops[MAXF];
+        int nf = 0;
+        src[nf] = N; ops[nf++] = OP_ZK0;
+        for (int d = 0; d < nm; ++d) { src[nf] = M[d]; ops[nf++] = OP_ID; }
+        inverse(nf, src, ops);
+        PWU<R> pw;
+        pw.ph = ph;
+        pw.nm = nm;
+        pw.nhat = N;
+        pw.status = &ctrl->status;
+        xpass(nf, nm, pw, xrb_io);
+        forward(nm, OA);
+        CombineU<R> c;
+        for (int q = 0; q < 6; ++q) { c.P[q] = P[q]; c.P0[q] = P0[q]; }
+        for (int d = 0; d < 3; ++d) c.U[d] = OA[std::min(d, nm - 1)];
+        combine_u_kernel<R><<<combine_grid(), 256, 0, st>>>(g, ph, nm, c, ctrl);
+        launches++;
+    }
+
+    int check_status()
+    {
+        unsigned stv = 0;
+        CK(cudaMemcpyAsync(&stv, &ctrl->status, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (stv) {
+            CK(cudaMemsetAsync(&ctrl->status, 0, sizeof(unsigned), st));
+            if (stv & ST_NONFINITE) { err = "state is not finite (NaN or Inf)"; return HYDFT_E_NONFINITE; }
+            if (stv & ST_NONPOS) {
+                err = "density became non-positive; reduce the amplitude or the time step";
+                return HYDFT_E_NONPOS;
+            }
+        }
+        return 0;
+    }
+
+    int64_t step_launches = 0;
+
+    int advance(int nsteps) override
+    {
+        if (nsteps <= 0) return 0;
+        if (!gexec) {
+            const int64_t before = launches;
+            CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            one_step();
+            cudaGraph_t gr = nullptr;
+            CK(cudaStreamEndCapture(st, &gr));
+            graph = gr;
+            step_launches = launches - before;
+            launches = before;
+            CK(cudaGraphInstantiate(&gexec, graph, 0));
+        }
+        for (int i = 0; i < nsteps; ++i) {
+            CK(cudaGraphLaunch(gexec, st));
+            launches += step_launches;
+        }
+        finish();
+        CK(cudaGetLastError());
+        return check_status();
+    }
+
+    int rhs(double t, double *dn, double *dmom, double *dpi) override
+    {
+        // t only enters through the external force: set the stage scalars of
+        // stage 0 at time t
+        double t0, dt0;
+        int64_t s0;
+        get_time(&t0, &dt0, &s0);
+        set_time(t, dt0);
+        begin_step();
+        phase_a(0, ph.evolve != 0);
+        phase_b(0, true);
+        set_time(t0, dt0);
+        CK(cudaGetLastError());
+        if (int rc = check_status()) return rc;
+        // outputs to real space
+        const cplx<R> *src[MAXF];
+        R *dsts[MAXF];
+        int nf = 0;
+        src[nf] = HN; dsts[nf++] = io_real;
+        for (int d = 0; d < 3; ++d) { src[nf] = HM[d]; dsts[nf++] = io_real + (1 + d) * ncell; }
+        if (int rc = to_real(nf, src, dsts)) return rc;
+        if (int rc = down(dn, io_real, 1, 0.0)) return rc;
+        if (int rc = down(dmom, io_real + ncell, 3, 0.0)) return rc;
+        if (ph.evolve && dpi) {
+            nf = 0;
+            for (int q = 0; q < 6; ++q) { src[nf] = HP[q]; dsts[nf++] = io_real + q * ncell; }
+            if (int rc = to_real(nf, src, dsts)) return rc;
+            if (int rc = down(dpi, io_real, 6, 0.0)) return rc;
+        }
+        return 0;
+    }
+
+    // compact fields -> real-space device arrays
+    int to_real(int nf, const cplx<R> *const *src, R *const *dst)
+    {
+        int ops[MAXF];
+        for (int f = 0; f < nf; ++f) ops[f] = OP_ID;
+        inverse(nf, src, ops);
+        PWToReal<R> pw;
+        for (int f = 0; f < MAXF; ++f) pw.dst[f] = f < nf ? dst[f] : nullptr;
+        pw.ncell = ncell;
+        xpass(nf, 0, pw, xrb_io);
+        CK(cudaGetLastError());
+        return 0;
+    }
+
+    // real-space device arrays -> compact fields (masked to the band)
+    int from_real(int nf, const R *const *src, cplx<R> *const *dst)
+    {
+        PWFromReal<R> pw;
+        for (int f = 0; f < MAXF; ++f) pw.src[f] = f < nf ? src[f] : nullptr;
+        pw.nf = nf;
+        xpass(0, nf, pw, xrb_io);
+        forward(nf, const_cast<cplx<R> *const *>(dst));
+        CK(cudaGetLastError());
+        return 0;
+    }
+
+    // device real (R) -> host double, ncomp fields
+    int down(double *h, const R *d, int ncomp, double add)
+    {
+        double *tmp;
+        const size_t n = ncomp * ncell;
+        CK(cudaMallocAsync((void **)&tmp, n * sizeof(double), st));
+        real_to_double_kernel<R><<<592, 256, 0, st>>>(tmp, d, add, n);
+        launches++;
+        CK(cudaMemcpyAsync(h, tmp, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaFreeAsync(tmp, st));
+        CK(cudaStreamSynchronize(st));
+        return 0;
+    }
+
+    int up(R *d, const double *h, int ncomp, double sub)
+    {
+        double *tmp;
+        const size_t n = ncomp * ncell;
+        CK(cudaMallocAsync((void **)&tmp, n * sizeof(double), st));
+        CK(cudaMemcpyAsync(tmp, h, n * sizeof(double), cudaMemcpyHostToDevice, st));
+        fill_real_kernel<R><<<592, 256, 0, st>>>(d, tmp, sub, n);
+        launches++;
+        CK(cudaFreeAsync(tmp, st));
+        return 0;
+    }
+
+    int set_state(const double *n, const double *mom, const double *pi) override
+    {
+        if (!n || !mom) { err = "set_state: n and mom are required"; return HYDFT_E_BAD; }
+        if (ph.evolve && !pi) { err = "set_state: pi is required for the Maxwell closure"; return HYDFT_E_BAD; }
+        // mean density in FP64 (the k = 0 mode), deviations transformed in R
+        double s = 0.0, c = 0.0;
+        for (size_t q = 0; q < ncell; ++q) {
+            const double v = n[q];
+            const double t = s + v;
+            if (std::fabs(s) >= std::fabs(v)) c += (s - t) + v; else c += (v - t) + s;
+            s = t;
+        }
+        const double nmean = (s + c) / (double)ncell;
+        if (int rc = up(io_real, n, 1, nmean)) return rc;
+        if (int rc = up(io_real + ncell, mom, 3, 0.0)) return rc;
+        const R *src[4] = {io_real, io_real + ncell, io_real + 2 * ncell, io_real + 3 * ncell};
+        cplx<R> *dst[4] = {N, M[0], M[1], M[2]};
+        if (int rc = from_real(4, src, dst)) return rc;
+        set_k0_kernel<R><<<1, 32, 0, st>>>(N, nmean);
+        launches++;
+        if (ph.evolve) {
+            if (int rc = up(io_real, pi, 6, 0.0)) return rc;
+            const R *sp[6];
+            cplx<R> *dp[6];
+            for (int q = 0; q < 6; ++q) { sp[q] = io_real + q * ncell; dp[q] = P[q]; }
+            if (int rc = from_real(6, sp, dp)) return rc;
+        }
+        CK(cudaMemsetAsync(&ctrl->pending, 0, sizeof(int), st));
+        CK(cudaStreamSynchronize(st));
+        return 0;
+    }
+
+    int get_state(double *n, double *mom, double *pi) override
+    {
+        double nmean = 0.0;
+        {
+            cplx<R> h0;
+            CK(cudaMemcpyAsync(&h0, N, sizeof(h0), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            nmean = (double)h0.x;
+        }
+        const cplx<R> *src[MAXF];
+        R *dsts[MAXF];
+        int nf = 0;
+        src[nf] = N; dsts[nf++] = io_real;
+        for (int d = 0; d < 3; ++d) { src[nf] = M[d]; dsts[nf++] = io_real + (1 + d) * ncell; }
+        // n without its mean, added back in FP64
+        {
+            int ops[MAXF];
+            ops[0] = OP_ZK0;
+            for (int f = 1; f < nf; ++f) ops[f] = OP_ID;
+            inverse(nf, src, ops);
+            PWToReal<R> pw;
+            for (int f = 0; f < MAXF; ++f) pw.dst[f] = f < nf ? dsts[f] : nullptr;
+            pw.ncell = ncell;
+            xpass(nf, 0, pw, xrb_io);
+        }
+        if (n) if (int rc = down(n, io_real, 1, nmean)) return rc;
+        if (mom) if (int rc = down(mom, io_real + ncell, 3, 0.0)) return rc;
+        if (ph.evolve && pi) {
+            nf = 0;
+            for (int q = 0; q < 6; ++q) { src[nf] = P[q]; dsts[nf++] = io_real + q * ncell; }
+            if (int rc = to_real(nf, src, dsts)) return rc;
+            if (int rc = down(pi, io_real, 6, 0.0)) return rc;
+        }
+        return 0;
+    }
+
+    int reductions(double *sum_n, double sum_m[3], double *sum_m2n, double *nmin, double *nmax,
+                   double *umax) override
+    {
+        const cplx<R> *src[4] = {N, M[0], M[1], M[2]};
+        int ops[4] = {OP_ZK0, OP_ID, OP_ID, OP_ID};
+        inverse(1 + nm, src, ops);
+        PWToReal<R> pw;
+        for (int f = 0; f < MAXF; ++f) pw.dst[f] = nullptr;
+        pw.dst[0] = io_real;
+        for (int d = 0; d < nm; ++d) pw.dst[1 + d] = io_real + (1 + d) * ncell;
+        pw.ncell = ncell;
+        xpass(1 + nm, 0, pw, xrb_io);
+        reduce_fields_kernel<R><<<red_blocks, 256, 0, st>>>(io_real, io_real + ncell, ncell, nm, N,
+                                                            ph.inv_mass, rpart);
+        reduce_final_kernel<R><<<1, 32, 0, st>>>(rpart, red_blocks, rout);
+        launches += 2;
+        RedPart h;
+        CK(cudaMemcpyAsync(&h, rout, sizeof(h), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        *sum_n = h.sn;
+        for (int d = 0; d < 3; ++d) sum_m[d] = d < nm ? h.sm[d] : 0.0;
+        *sum_m2n = h.sk;
+        *nmin = h.nmin;
+        *nmax = h.nmax;
+        *umax = h.umax;
+        return 0;
+    }
+
+    int mode(int field, int mx, int my, int mz, double *re, double *im) override
+    {
+        // the state is dealiased: coefficients outside the band are zero
+        const cplx<R> *f = field == 0 ? N : M[field - 1];
+        bool conjugate = false;
+        if (mx < 0) { mx = -mx; my = -my; mz = -mz; conjugate = true; }
+        // wrap to the signed range of each axis
+        auto wrapm = [](int m, int n) { m = ((m % n) + n) % n; return m <= n / 2 ? m : m - n; };
+        my = g.ny > 1 ? wrapm(my, g.ny) : 0;
+        mz = g.nz > 1 ? wrapm(mz, g.nz) : 0;
+        if (mx > g.Mx || std::abs(my) > g.My || std::abs(mz) > g.Mz) {
+            *re = 0.0;
+            *im = 0.0;
+            return 0;
+        }
+        const int kyc = my >= 0 ? my : my + 2 * g.My + 1;
+        const int kzc = mz >= 0 ? mz : mz + 2 * g.Mz + 1;
+        cplx<R> h;
+        CK(cudaMemcpyAsync(&h, f + ((size_t)kzc * g.nkyc + kyc) * g.pkx + mx, sizeof(h), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        *re = (double)h.x;
+        *im = conjugate ? -(double)h.y : (double)h.y;
+        return 0;
+    }
+
+    void set_time(double t, double dt) override
+    {
+        Ctrl c;
+        cudaMemcpyAsync(&c, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st);
+        cudaStreamSynchronize(st);
+        c.t = t;
+        c.dt = dt;
+        cudaMemcpyAsync(ctrl, &c, sizeof(Ctrl), cudaMemcpyHostToDevice, st);
+        cudaStreamSynchronize(st);
+    }
+
+    void get_time(double *t, double *dt, int64_t *step) override
+    {
+        Ctrl c;
+        cudaMemcpyAsync(&c, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st);
+        cudaStreamSynchronize(st);
+        if (t) *t = c.t;
+        if (dt) *dt = c.dt;
+        if (step) *step = c.step;
+    }
+};
+
+SolverBase *make_solver(const SolverSetup &s, int precision, int device, std::string &err)
+{
+    SolverBase *r = nullptr;
+    int rc = 0;
+    if (precision == 32) {
+        auto *p = new Solver<float>();
+        rc = p->init(s, device);
+        r = p;
+    } else {
+        auto *p = new Solver<double>();
+        rc = p->init(s, device);
+        r = p;
+    }
+    if (rc) {
+        err = r->err;
+        delete r;
+        return nullptr;
+    }
+    return r;
+}
+
+}  // namespace hydft

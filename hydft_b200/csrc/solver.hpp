@@ -1,0 +1,63 @@
+// Host-side interface of the device solver (one simulation on one GPU).
+#pragma once
+
+#include <complex>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace hydft {
+
+struct Phys;  // kernels.cuh
+
+// Everything the solver needs, computed by the host setup (setup.cpp).
+struct SolverSetup {
+    Grid g;
+    int nm = 1;                       // momentum components evolved (= ndim)
+    // physics constants (mirrors Phys in kernels.cuh)
+    double beta = 3, mass = 1, n0 = 0;
+    int term_order[8] = {0};
+    int nterms_local = 0;
+    double cn = 0, cg = 0, alpha_ref = 0;
+    int evolve = 0, newtonian = 0;
+    double eta = 0, xi = 0, tau = 0;
+    int ext_active = 0, ext_kind = 0, ext_td = 0;
+    double ext_k[3] = {0, 0, 0}, ext_amp = 0, ext_omega = 0, ext_ramp = 0;
+    int drive_in_band = 0, drive_idx = 0, drive_conj = 0;
+    double volume = 1;
+    std::vector<double> klin;         // compact band, sum of hartree/ry mu kernels
+    std::vector<double> fdtab;        // 6*6601, electrons only
+    std::vector<std::complex<double>> ex, ey, ez;
+    std::vector<double> gauss_f;      // gaussian external force (3 real fields), optional
+};
+
+class SolverBase {
+public:
+    virtual ~SolverBase() {}
+    virtual int set_state(const double *n, const double *mom, const double *pi) = 0;
+    virtual int get_state(double *n, double *mom, double *pi) = 0;
+    virtual int advance(int nsteps) = 0;
+    virtual int rhs(double t, double *dn, double *dmom, double *dpi) = 0;
+    // FP64 compensated sums over the grid
+    virtual int reductions(double *sum_n, double sum_m[3], double *sum_m2n, double *nmin,
+                           double *nmax, double *umax) = 0;
+    virtual int mode(int field, int mx, int my, int mz, double *re, double *im) = 0;
+    virtual void set_time(double t, double dt) = 0;
+    virtual void get_time(double *t, double *dt, int64_t *step) = 0;
+    virtual void *stream() = 0;
+    virtual int precision_bits() const = 0;
+    // drive frequency of the external potential (model_t%ext%omega); the
+    // captured step graph is rebuilt on the next advance
+    virtual void set_ext_omega(double w) = 0;
+    // the host-side setup constants in use
+    virtual const SolverSetup &setup() const = 0;
+    int64_t launches = 0;
+    std::string err;
+};
+
+// precision: 64 or 32.  Returns nullptr and fills err on failure.
+SolverBase *make_solver(const SolverSetup &s, int precision, int device, std::string &err);
+
+}  // namespace hydft

@@ -1,0 +1,213 @@
+/*
+ * hydft_gpu.h -- C ABI of the B200 (sm_100a) implementation of HyDFT's
+ * nonlinear pseudo-spectral solver step.
+ *
+ * The library replaces `model_t%advance` / `model_t%rhs` of HyDFT
+ * (src/model/model.f90:85-227) and the setup it depends on (species build,
+ * OZ-HNC c(k), Fermi-Dirac tables).  Every entry point is `extern "C"`,
+ * takes plain pointers and sizes, returns an int status (HYDFT_OK = 0) and
+ * never aborts: where the reference calls `fatal` (src/core/kinds.f90:26-30)
+ * the library returns a non-zero code and hydft_gpu_last_error() gives the
+ * message, so a Fortran shim can keep the reference's behaviour by calling
+ * `fatal` itself.
+ *
+ * Field arrays on the host use the reference's Fortran order: n(nx,ny,nz)
+ * with x fastest; mom(nx,ny,nz,3) and pi(nx,ny,nz,6) with the component index
+ * slowest (Pi components xx,yy,zz,xy,xz,yz as in src/closure/stress.f90:7).
+ *
+ * One handle belongs to one host thread; calls on it are not re-entrant.
+ */
+#ifndef HYDFT_GPU_H
+#define HYDFT_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+enum {
+    HYDFT_OK = 0,
+    HYDFT_ERR_BAD_ARG = 1,             /* invalid parameter or size */
+    HYDFT_ERR_OOM = 2,                 /* device allocation failed */
+    HYDFT_ERR_NONPOSITIVE_DENSITY = 3, /* model.f90:91, fe_*.f90 positivity checks */
+    HYDFT_ERR_NONFINITE = 4,           /* NaN/Inf in the state */
+    HYDFT_ERR_NEWTON = 5,              /* Fermi-Dirac inverse did not converge */
+    HYDFT_ERR_TIMEOUT = 6,             /* a bounded device wait ran out */
+    HYDFT_ERR_CUDA = 7,                /* CUDA runtime error */
+    HYDFT_ERR_UNSUPPORTED = 8,         /* option the GPU path does not implement */
+    HYDFT_ERR_HNC = 9,                 /* structure: HNC failed (structure_source.f90:63) */
+    HYDFT_ERR_IO = 10,                 /* cannot read an input file */
+    HYDFT_ERR_CFL = 11                 /* compute_dt cannot determine a step (model.f90:180) */
+};
+
+/*
+ * Run-time parameters: the reference's params_t (src/core/params.f90:17-78)
+ * as a POD struct.  Strings are NUL-terminated, lower case.  Fields of the
+ * namelists the solver step does not use (&linear, &output) are kept so the
+ * struct round-trips an input file.  `gpu_precision` is new ("fp64" or
+ * "fp32"), read from an optional &gpu namelist that the reference ignores.
+ */
+typedef struct hydft_params {
+    /* &grid */
+    int nx, ny, nz;
+    double lx, ly, lz;
+    int dealias;
+    /* &species */
+    char kind[16];            /* "ion" | "electron" */
+    double gamma, kappa, rs, theta, mass;
+    char terms[64];           /* comma list of ideal, tf, gradient, hartree, ry */
+    double tfk_gamma;
+    char closure[16];         /* "newtonian" | "maxwell" */
+    char transport[16];       /* "constant" | "yukawa_fit" | "stanton_murillo" | "electron_fit" */
+    double eta, xi, tau;
+    char tau_model[16];       /* "ichimaru" | "constant" */
+    double adiabatic_index;
+    char structure[16];       /* "hnc" | "file" | "none" */
+    char structure_file[256];
+    char structure_kind[4];   /* "s" | "c" */
+    /* &hnc */
+    int hnc_nr, hnc_maxiter;
+    double hnc_rmax, hnc_tol, hnc_mix;
+    /* &time */
+    double dt, cfl, tend;
+    int nsteps_max, iout, iprobe, idiag;
+    /* &initial */
+    char ic[16];
+    double ic_amplitude;
+    int ic_mode[3];
+    double ic_width;
+    int ic_seed;
+    /* &external */
+    char vext[16];            /* "none" | "mode" | "driven" | "gaussian" */
+    double vext_amplitude;
+    int vext_mode[3];
+    double vext_omega, vext_width, vext_ramp;
+    /* &probe */
+    int probe_mode[3];
+    /* &output */
+    char prefix[256];
+    /* &gpu (new) */
+    char gpu_precision[8];    /* "fp64" | "fp32" */
+} hydft_params;
+
+/* Defaults of params_t (src/core/params.f90:17-78) and "fp64". */
+int hydft_params_default(hydft_params *p);
+
+/* params_t%read (src/core/params.f90:82-180): read the namelists from
+ * `path` over the values already in *p, then apply the derived defaults
+ * (terms per kind, Gamma from rs and theta, kappa = 0 for electrons). */
+int hydft_params_read(const char *path, hydft_params *p);
+
+/* The derived defaults of params_read (params.f90:161-172) alone, for
+ * callers that fill the struct in code as the reference's tests do. */
+int hydft_params_finalize(hydft_params *p);
+
+/* An optional structure table c(k) on increasing k > 0 that replaces the
+ * HNC solve (the 'file' source, structure_source.f90:87-138, or a table
+ * computed elsewhere).  u_ex / du_dgamma feed tau_model = 'ichimaru'. */
+typedef struct hydft_structure {
+    int n;
+    const double *k;
+    const double *c;
+    double u_ex, du_dgamma;
+    int has_energy;
+} hydft_structure;
+
+typedef struct hydft_gpu hydft_gpu;
+
+/*
+ * model_t%init (src/model/model.f90:56-74): grid, species build (units,
+ * structure, functional terms, transport, stress closure), state allocation
+ * (n = n0, mom = 0, Pi = 0) and the external potential.  With st == NULL
+ * and p->structure == "hnc" the OZ-HNC equation is solved on the GPU in
+ * FP64.  `device` selects the CUDA device.
+ */
+int hydft_gpu_create(const hydft_params *p, const hydft_structure *st, int device,
+                     hydft_gpu **out);
+void hydft_gpu_destroy(hydft_gpu *h);
+const char *hydft_gpu_last_error(const hydft_gpu *h);
+/* message of the last failed hydft_gpu_create on this thread */
+const char *hydft_gpu_create_error(void);
+
+/* Copy the state in / out (host arrays, Fortran order).  pi may be NULL
+ * unless the Maxwell closure evolves Pi.  set_state projects the fields onto
+ * the dealiased band, as the reference's state is after every stage. */
+int hydft_gpu_set_state(hydft_gpu *h, const double *n, const double *mom, const double *pi);
+int hydft_gpu_get_state(hydft_gpu *h, double *n, double *mom, double *pi);
+
+/* set_initial_condition (src/model/initial.f90:23-75): kind "uniform",
+ * "mode", "gaussian", or "random" (seeded counter-based stream in place of
+ * gfortran's generator).  Resets mom and Pi to zero. */
+int hydft_gpu_set_initial_condition(hydft_gpu *h, const char *kind, double amplitude,
+                                    const int mode[3], double width, int seed);
+
+/* nsteps calls of model_t%advance (model.f90:186-227) at the current dt. */
+int hydft_gpu_advance(hydft_gpu *h, int nsteps);
+
+/* model_t%rhs (model.f90:85-146) of the current state at time t; outputs
+ * are host arrays (dpi may be NULL unless Pi evolves). */
+int hydft_gpu_rhs(hydft_gpu *h, double t, double *dn, double *dmom, double *dpi);
+
+/* model_t%compute_dt (model.f90:150-183); the result is also the dt that
+ * the next advance uses. */
+int hydft_gpu_compute_dt(hydft_gpu *h, double *dt);
+
+/* Scalars of model_t: t, dt, step. */
+int hydft_gpu_get_time(const hydft_gpu *h, double *t, double *dt, int64_t *step);
+int hydft_gpu_set_time(hydft_gpu *h, double t, double dt);
+
+/* diag_t%budgets (src/model/diagnostics.f90:41-60): mass, momentum and
+ * kinetic energy from FP64 compensated sums over the grid; free energy of
+ * the functional (+ external potential).  nmin/nmax as in diag_write. */
+int hydft_gpu_budgets(hydft_gpu *h, double *mass, double mom[3], double *ekin, double *fe,
+                      double *nmin, double *nmax);
+
+/* spec_t%mode (spectral.f90:179-188) of n (field 0) or mom_1..3 (1..3). */
+int hydft_gpu_mode(hydft_gpu *h, int field, int mx, int my, int mz, double *re, double *im);
+
+/* Setup scalars (units, transport, stress): name in
+ * n0 beta gamma kappa mass hbar theta alpha0 cn lambda_qsp lambda_tf eta xi
+ * tau eta_l u_ex du_dgamma kmax_dealiased volume cg ndim evolve precision. */
+int hydft_gpu_get_scalar(const hydft_gpu *h, const char *name, double *value);
+int hydft_gpu_set_scalar(hydft_gpu *h, const char *name, double value);
+
+/* The structure table in use (k, c(k)); n is the table length. */
+int hydft_gpu_get_structure(const hydft_gpu *h, int *n, double *k, double *c);
+
+/* Total linear kernel K(k) = sum of the terms' kernels (functional.f90:72-80). */
+int hydft_gpu_kernel(const hydft_gpu *h, double k, double *kk);
+
+/* The device stream the handle launches on (cudaStream_t as void*). */
+void *hydft_gpu_stream(const hydft_gpu *h);
+
+/* Kernel launches made by the library since creation (for accounting). */
+int64_t hydft_gpu_launch_count(const hydft_gpu *h);
+
+/* ------------------------------------------------- setup on the device */
+
+/*
+ * OZ-HNC solve (src/structure/oz_hnc.f90:111-296, hnc_solve with its
+ * Gamma continuation) in FP64 on the GPU.  potential: "yukawa", "coulomb",
+ * "hansen_mcdonald".  Outputs (length nr, any may be NULL): r, k, g(r),
+ * c(k), S(k); scalars u_ex, converged, niter, residual.
+ */
+int hydft_gpu_hnc_solve(const char *potential, double gamma, double kappa, double lambda,
+                        double n0, int nr, double rmax, double tol, double mix, int maxiter,
+                        int device, double *r, double *k, double *g, double *ck, double *sk,
+                        double *u_ex, int *converged, int *niter, double *residual);
+
+/* Fermi-Dirac table tab(6, 6601) (fermi_dirac.f90:30-74) built on the GPU;
+ * out has 6*6601 doubles, column index fastest. */
+int hydft_gpu_fd_table(int device, double *out, int *ntab);
+
+/* Batched Fermi-Dirac inverse alpha = I_{1/2}^{-1}(y) (fermi_dirac.f90:241-267)
+ * on the GPU for n host values. */
+int hydft_gpu_fd_alpha(int device, const double *y, double *alpha, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HYDFT_GPU_H */

@@ -1,0 +1,212 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+FP64: every result within 1e-10 relative (l2 over each field) of the oracle
+on the same seeded inputs and the same structure table c(k).  FP32: within
+1e-5.  The oracle restates the reference's FP64 FFTW path; see oracle/.
+"""
+import numpy as np
+import pytest
+
+from hydft_b200 import ic
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-10
+TOL32 = 1e-5
+
+
+def rel(a, b):
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
+
+
+@pytest.fixture(scope="module")
+def hg():
+    import hydft_b200
+    hydft_b200.lib()
+    return hydft_b200
+
+
+def pair(hg, orc, **kw):
+    """A GPU model and an oracle model on the GPU's structure table."""
+    m = hg.Model(hg.default_params(**kw))
+    k, c = m.structure()
+    st = None
+    if k.size:
+        st = orc.Structure(k, c, m.scalar("n0"), m.scalar("u_ex"), m.scalar("du_dgamma"), True)
+    okw = {kk: v for kk, v in kw.items() if kk != "gpu_precision"}
+    return m, orc.Model(orc.params(**okw), st)
+
+
+def seeded_state(m, amp=0.02, seed=5, with_mom=True, with_pi=True):
+    nx, ny, nz = m.nx, m.ny, m.nz
+    p = m.p
+    n0 = m.scalar("n0")
+    n = n0 * (1 + amp * ic.random_field(nx, ny, nz, p.lx, p.ly, p.lz, seed))
+    mom = np.zeros((3, nz, ny, nx))
+    if with_mom:
+        for d in range(m.scalar("ndim").__int__()):
+            mom[d] = 0.01 * n0 * ic.random_field(nx, ny, nz, p.lx, p.ly, p.lz, seed + 10 + d)
+    pi = None
+    if m.has_pi and with_pi:
+        pi = np.zeros((6, nz, ny, nx))
+        for c in range(6):
+            pi[c] = 1e-3 * ic.random_field(nx, ny, nz, p.lx, p.ly, p.lz, seed + 20 + c)
+        if m.scalar("ndim") < 3:
+            pass
+    return n, mom, pi
+
+
+ION = dict(kind="ion", gamma=10.0, kappa=1.0, hnc_nr=2048, hnc_rmax=40.0, transport="yukawa_fit")
+ELEC = dict(kind="electron", rs=1.0, theta=1.0, hnc_nr=2048, hnc_rmax=40.0, transport="constant",
+            eta=0.2)
+
+
+def test_fd_table_and_inverse(hg, orc):
+    t = hg.fd_table()
+    to = orc.fd_table()
+    assert t.shape == to.shape == (6601, 6)
+    assert np.abs(t - to).max() / np.abs(to).max() < 1e-13
+    a = np.linspace(-35.0, 320.0, 97)
+    y = np.array([orc.fd("ip12", v) for v in a])
+    al = hg.fd_alpha(y)
+    ao = np.array([orc.fd_alpha_from_ip12(v)[0] for v in y])
+    assert np.abs(al - ao).max() < 1e-9 * max(1.0, np.abs(ao).max())
+
+
+@pytest.mark.parametrize("pot,gam,kap,lam", [("yukawa", 10.0, 1.0, 1.0), ("coulomb", 10.0, 0.0, 1.0),
+                                             ("hansen_mcdonald", 0.5, 0.0, 2 * np.sqrt(np.pi * 0.5))])
+def test_hnc_matches_oracle(hg, orc, pot, gam, kap, lam):
+    n0 = 3 / (4 * np.pi)
+    g = hg.hnc_solve(pot, gam, kap, lam, n0, 4096, 60.0, 1e-9, 0.2, 5000)
+    o = orc.hnc_solve(orc.make_pot(pot, gam, kap, lam), n0, 4096, 60.0, 1e-9, 0.2, 5000)
+    assert g["converged"] and o.converged
+    # both iterate to the 1e-9 residual tolerance; the DST summation order differs
+    assert np.abs(g["ck"] - o.ck).max() / np.abs(o.ck).max() < 1e-7
+    assert abs(g["u_ex"] - o.u_ex) < 1e-7 * abs(o.u_ex)
+
+
+CASES = {
+    "ion_newtonian_3d": dict(ION, nx=16, ny=12, nz=8, lx=20.0, ly=15.0, lz=10.0, closure="newtonian"),
+    "ion_maxwell_3d": dict(ION, nx=16, ny=8, nz=12, lx=20.0, ly=10.0, lz=15.0, closure="maxwell",
+                           tau_model="constant", tau=1.5),
+    "ion_maxwell_ichimaru": dict(ION, nx=12, ny=12, nz=12, lx=15.0, ly=15.0, lz=15.0, gamma=50.0,
+                                 kappa=2.0, closure="maxwell", tau_model="ichimaru"),
+    "electron_driven_3d": dict(ELEC, nx=16, ny=8, nz=8, lx=20.0, ly=10.0, lz=10.0, closure="newtonian",
+                               vext="driven", vext_amplitude=1e-3, vext_mode=(2, 1, 0),
+                               vext_omega=0.9, vext_ramp=0.05),
+    "ion_1d": dict(ION, nx=32, ny=1, nz=1, lx=20.0, closure="newtonian", gamma=2.0, kappa=0.1,
+                   transport="constant", eta=0.3),
+    "ion_2d_maxwell": dict(ION, nx=32, ny=4, nz=1, lx=20.0, ly=5.0, closure="maxwell",
+                           tau_model="constant", tau=2.0, transport="constant", eta=0.2),
+    "ion_nodealias_mode": dict(ION, nx=24, ny=6, nz=6, lx=20.0, ly=5.0, lz=5.0, dealias=False,
+                               vext="mode", vext_amplitude=1e-3, vext_mode=(1, 1, 1), eta=0.4,
+                               transport="constant"),
+}
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_rhs_fp64(hg, orc, case):
+    m, o = pair(hg, orc, dt=0.01, **CASES[case])
+    n, mom, pi = seeded_state(m)
+    m.set_state(n, mom, pi)
+    o.set_state(n, mom, pi)
+    # the oracle projects nothing: hand it the GPU's dealiased state
+    n2, mom2, pi2 = m.get_state()
+    assert rel(n2, n) < 1e-12
+    o.set_state(n2, mom2, pi2)
+    t = 0.37
+    dn, dmom, dpi = m.rhs(t)
+    on, omom, opi = o.rhs(t)
+    assert rel(dn, on) < TOL64, rel(dn, on)
+    assert rel(dmom, omom) < TOL64, rel(dmom, omom)
+    if m.has_pi:
+        assert rel(dpi, opi) < TOL64, rel(dpi, opi)
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_advance_fp64(hg, orc, case):
+    m, o = pair(hg, orc, dt=0.02, **CASES[case])
+    n, mom, pi = seeded_state(m)
+    m.set_state(n, mom, pi)
+    n2, mom2, pi2 = m.get_state()
+    o.set_state(n2, mom2, pi2)
+    m.advance(5)
+    o.advance(5)
+    g = m.get_state()
+    assert abs(m.t - o.t) < 1e-14 and m.step == 5
+    assert rel(g[0], o.n) < TOL64, rel(g[0], o.n)
+    assert rel(g[0] - g[0].mean(), o.n - o.n.mean()) < 1e-9
+    assert rel(g[1], o.mom) < TOL64, rel(g[1], o.mom)
+    if m.has_pi:
+        assert rel(g[2], o.pi) < TOL64, rel(g[2], o.pi)
+
+
+@pytest.mark.parametrize("case", ["ion_newtonian_3d", "ion_maxwell_3d", "electron_driven_3d"])
+def test_advance_fp32(hg, orc, case):
+    m, o = pair(hg, orc, dt=0.02, gpu_precision="fp32", **CASES[case])
+    n, mom, pi = seeded_state(m)
+    m.set_state(n, mom, pi)
+    n2, mom2, pi2 = m.get_state()
+    o.set_state(n2, mom2, pi2)
+    m.advance(20)
+    o.advance(20)
+    g = m.get_state()
+    assert rel(g[0], o.n) < TOL32
+    assert rel(g[1], o.mom) < TOL32, rel(g[1], o.mom)
+    if m.has_pi:
+        assert rel(g[2], o.pi) < TOL32, rel(g[2], o.pi)
+
+
+def test_budgets_and_mode(hg, orc):
+    m, o = pair(hg, orc, dt=0.02, **CASES["ion_newtonian_3d"])
+    n, mom, _ = seeded_state(m)
+    m.set_state(n, mom)
+    n2, mom2, _ = m.get_state()
+    o.set_state(n2, mom2)
+    mass, mm, ek, fe, nmin, nmax = m.budgets()
+    omass, omm, oek, ofe = o.budgets()
+    assert abs(mass / omass - 1) < 1e-13
+    assert np.abs(mm - omm).max() < 1e-13 * omass
+    assert abs(ek / oek - 1) < 1e-12
+    assert abs(nmin - n2.min()) < 1e-14 and abs(nmax - n2.max()) < 1e-14
+    # spec_mode takes mx >= 0 (spectral.f90:179-188); a negative mx is
+    # answered with the conjugate of mode (-mx,-my,-mz)
+    for (mx, my, mz) in [(1, 0, 0), (2, -1, 3), (0, 2, -2), (-1, 1, 1), (7, 0, 0)]:
+        for f, arr in ((0, n2), (1, mom2[0]), (2, mom2[1])):
+            ref = o.mode(arr, mx, my, mz) if mx >= 0 else np.conj(o.mode(arr, -mx, -my, -mz))
+            assert abs(m.mode(f, mx, my, mz) - ref) < 1e-15 + 1e-12 * abs(ref)
+
+
+def test_compute_dt_matches_oracle(hg, orc):
+    kw = dict(CASES["ion_newtonian_3d"])
+    kw.update(dt=0.0, cfl=0.3)
+    m, o = pair(hg, orc, **kw)
+    n, mom, _ = seeded_state(m)
+    m.set_state(n, mom)
+    n2, mom2, _ = m.get_state()
+    o.set_state(n2, mom2)
+    assert abs(m.compute_dt() / o.compute_dt() - 1) < 1e-12
+
+
+def test_initial_conditions(hg, orc):
+    kw = dict(CASES["ion_newtonian_3d"])
+    m, o = pair(hg, orc, dt=0.02, **kw)
+    for kind in ("mode", "gaussian", "uniform"):
+        m.set_initial_condition(kind, 1e-3, (2, 1, 0), 2.0)
+        o.set_ic(kind, 1e-3, (2, 1, 0), 2.0)
+        assert rel(m.n, o.n) < 1e-13, kind
+    m.set_initial_condition("random", 0.02, seed=7)
+    d = ic.random_field(16, 12, 8, 20.0, 15.0, 10.0, seed=7)
+    assert rel(m.n, m.scalar("n0") * (1 + 0.02 * d)) < 1e-13
+
+
+def test_nonpositive_density_is_an_error(hg):
+    m = hg.Model(hg.default_params(dt=0.5, **CASES["ion_1d"]))
+    n0 = m.scalar("n0")
+    x = np.arange(32) * 20.0 / 32
+    n = n0 * (1 + 0.95 * np.cos(2 * np.pi * x / 20.0)).reshape(1, 1, 32)
+    m.set_state(n, np.zeros((3, 1, 1, 32)) + 0.3 * n0)
+    with pytest.raises(hg.HydftError) as e:
+        m.advance(50)
+    assert e.value.code in (3, 4)
