@@ -1,0 +1,373 @@
+"""Benchmark of the HyDFT solver step on B200.
+
+Workload (one "step" = one low-storage RK3 step, 3 stages, of the whole
+grid): Yukawa ions with the Maxwell closure, tau from the Ichimaru form
+(HNC u_ex and du/dGamma), 256^3 periodic box L = 64 a, Gamma = 50,
+kappa = 2, eta from the Bastea MD fit, Gaussian random delta n with power
+spectrum ~ exp(-q^2), rms 1e-2 (seeded counter-based stream), u = 0,
+Pi = 0; fields in FP32 with FP64 conserved sums.  The FP64 path is timed
+beside it ("FP32 vs FP64-plain"), and the FP32 field error is measured
+against the FP64 run after the timed steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs independent replicas, one per GPU (the solver step does not
+shard; no collective is on the data path).  --impl reference times the
+reference algorithm's CPU path (the FP64 oracle restatement of the
+Fortran code, OpenMP over all host cores) on a bounded sample of the same
+workload.  One JSON line is printed by rank 0.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RK3 cell-steps/s FP32-batched vs FP64-plain on B200 at ≤1e-5 rel err; p50/p99"
+UNIT = "cell-steps/s"
+# algorithmic bytes per cell-step of the minimal exact transform schedule,
+# Maxwell ions: 3 stages x (8 B x 44 transforms + 16 B x 10 state fields), FP32
+STEP_BYTES_FP32 = 3 * (8 * 44 + 16 * 10)
+
+
+def workload_params(hg, n, precision, L=64.0):
+    return hg.default_params(
+        kind="ion", gamma=50.0, kappa=2.0, nx=n, ny=n, nz=n, lx=L, ly=L, lz=L,
+        closure="maxwell", transport="yukawa_fit", tau_model="ichimaru",
+        hnc_nr=4096, hnc_rmax=80.0, cfl=0.4, dt=0.0, gpu_precision=precision)
+
+
+def initial_density(n, L, n0, seed=2024):
+    from hydft_b200 import ic
+    d = ic.gaussian_spectrum_field(n, n, n, L, L, L, seed, qc=1.0)
+    return n0 * (1.0 + 1e-2 * d)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profile_traffic(kernel, precision):
+    """dram bytes per launch of `kernel` from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "maxwell256_%s_kernels.md" % precision)
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("| %s |" % kernel):
+                    cols = [c.strip() for c in line.strip().strip("|").split("|")]
+                    return float(cols[-1])
+    except (OSError, ValueError, IndexError):
+        pass
+    return None
+
+
+def cpu_baseline(structure, threads, steps, n=64):
+    """The FP64 oracle (reference algorithm, CPU) on a 64^3 sample of the
+    workload: same physics and resolution (L scaled with N)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    L = 64.0 * n / 256.0
+    orc.set_threads(threads)
+    p = orc.params(kind="ion", gamma=50.0, kappa=2.0, nx=n, ny=n, nz=n, lx=L, ly=L, lz=L,
+                   closure="maxwell", transport="yukawa_fit", tau_model="ichimaru", cfl=0.4)
+    st = orc.Structure(structure["k"], structure["c"], 3 / (4 * np.pi), structure["u_ex"],
+                       structure["du_dgamma"], True)
+    m = orc.Model(p, st)
+    m.set_state(initial_density(n, L, 3 / (4 * np.pi)))
+    m.compute_dt()
+    m.advance(1)       # warm-up (plans, page faults)
+    t0 = time.perf_counter()
+    m.advance(steps)
+    el = time.perf_counter() - t0
+    return n ** 3 * steps / el, el
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import hydft_b200 as hg   # only for the HNC structure table of the workload
+    threads = os.cpu_count() or 1
+    try:
+        st = structure_for_workload(hg, device=0)
+    except Exception:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as orc
+        n0 = 3 / (4 * np.pi)
+        pot = orc.make_pot("yukawa", 50.0, 2.0)
+        s = orc.structure_from_hnc(pot, n0, 4096, 80.0, 1e-9, 0.2, 20000, with_derivative=True)
+        st = dict(k=s.k, c=s.c, u_ex=s.u_ex, du_dgamma=s.du_dgamma)
+    steps = max(1, args.steps)
+    v, el = cpu_baseline(st, threads, steps, n=args.ref_n)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "maxwell_ion_256^3 (sampled at %d^3)" % args.ref_n, "grid": args.ref_n,
+                       "steps_per_sample": steps},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": "%d^3 Maxwell ions, same physics and dx (L=%g), %d RK3 steps, "
+                                       "FP64 oracle restatement of the reference CPU path, OpenMP %d threads"
+                                       % (args.ref_n, 64.0 * args.ref_n / 256, steps, threads)},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def structure_for_workload(hg, device):
+    m = hg.Model(workload_params(hg, 8, "fp64"), device=device)
+    k, c = m.structure()
+    st = dict(k=k, c=c, u_ex=m.scalar("u_ex"), du_dgamma=m.scalar("du_dgamma"))
+    m.close()
+    return st
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--ref-n", type=int, default=64)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-plain leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import hydft_b200 as hg
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = local
+
+    n = args.n
+    L = 64.0
+    st = structure_for_workload(hg, dev)
+    m32 = hg.Model(workload_params(hg, n, "fp32"), structure=st, device=dev)
+    n0 = m32.scalar("n0")
+    nin = initial_density(n, L, n0)
+    zeros3 = np.zeros((3, n, n, n))
+    zeros6 = np.zeros((6, n, n, n))
+    m32.set_state(nin, zeros3, zeros6)
+    dt = m32.compute_dt()
+    stream = torch.cuda.ExternalStream(m32.stream_ptr(), device=dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # warm-up (graph capture, first touches)
+    m32.advance(args.warmup)
+    torch.cuda.synchronize(dev)
+    barrier()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    time.sleep(0.4)
+    launches0 = m32.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    barrier()
+    e0.record(stream)
+    m32.advance(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    gpu_launches = m32.launch_count() - launches0
+    ms_max = ms
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    cells = float(n) ** 3
+    value = cells * args.steps * world / (ms_max * 1e-3)
+    ms_step = ms_max / args.steps
+
+    # per-kernel device time of 2 uncaptured steps, CUDA events on the stream
+    prof = m32.profile(2)
+    tot = sum(v[0] for v in prof.values())
+    dom = max(prof.items(), key=lambda kv: kv[1][0])
+    dname, (dms, dbytes, dn) = dom
+    peak, peak_kind = measured_peak()
+    achieved = dbytes / (dms / dn * 1e-3) / 1e9
+    roof = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": peak_kind, "share": dms / tot,
+            "bytes_per_launch": dbytes, "avg_launch_ms": dms / dn,
+            "traffic": profile_traffic(dname, "fp32")}
+    kernels = {k: {"ms_per_step": v[0] / 2, "launches_per_step": v[2] / 2,
+                   "GBps": (v[1] / (v[0] / v[2] * 1e-3) / 1e9) if v[0] > 0 and v[1] > 0 else None}
+               for k, v in prof.items()}
+
+    extra = {}
+    # FP64-plain leg and the FP32 field error against it
+    if not args.no_fp64:
+        m64 = hg.Model(workload_params(hg, n, "fp64"), structure=st, device=dev)
+        m64.set_state(nin, zeros3, zeros6)
+        m64.set_time(0.0, dt)
+        s64 = torch.cuda.ExternalStream(m64.stream_ptr(), device=dev)
+        k64 = max(2, args.steps // 4)
+        m64.advance(1)
+        torch.cuda.synchronize(dev)
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(s64)
+        m64.advance(k64)
+        f1.record(s64)
+        torch.cuda.synchronize(dev)
+        v64 = cells * k64 / (f0.elapsed_time(f1) * 1e-3)
+        # same number of steps from the same state for the error
+        m32b = hg.Model(workload_params(hg, n, "fp32"), structure=st, device=dev)
+        m32b.set_state(nin, zeros3, zeros6)
+        m32b.set_time(0.0, dt)
+        m32b.advance(1 + k64)
+        a = m32b.get_state()
+        b = m64.get_state()
+        errs = {}
+        for name, x, y in (("n", a[0], b[0]), ("mom", a[1], b[1]), ("pi", a[2], b[2])):
+            errs[name] = float(np.linalg.norm(x - y) / np.linalg.norm(y))
+        errs["dn"] = float(np.linalg.norm((a[0] - n0) - (b[0] - n0)) / np.linalg.norm(b[0] - n0))
+        extra["fp64_plain"] = {"value": v64, "unit": UNIT, "ratio_fp32_over_fp64": value / world / v64}
+        extra["fp32_rel_err_vs_fp64"] = dict(errs, steps=1 + k64)
+        m64.close()
+        m32b.close()
+
+    # end to end through the public API: host arrays in, per-step advance()
+    # calls with a probe of one mode read back each step (the driver's loop,
+    # src/hydft.f90:41-51), the final state read back
+    me = hg.Model(workload_params(hg, n, "fp32"), structure=st, device=dev)
+    host_n = np.ascontiguousarray(nin)
+    torch.cuda.synchronize(dev)
+    barrier()
+    t0 = time.perf_counter()
+    me.set_state(host_n, zeros3, zeros6)
+    me.set_time(0.0, dt)
+    for _ in range(args.steps):
+        me.advance(1)
+        me.mode(0, 1, 0, 0)
+    fin = me.get_state()
+    torch.cuda.synchronize(dev)
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    state_bytes = 8 * (1 + 3 + 6) * cells
+    e2e = {"value": cells * args.steps * world / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": state_bytes / args.steps,
+           "d2h_bytes_per_step": 16 + state_bytes / args.steps}
+    me.close()
+    del fin
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, el = cpu_baseline(st, 1, 1, n=64)
+        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": "64^3 Maxwell ions, same physics and dx (L=16), 1 RK3 step (%.1f s), "
+                         "FP64 oracle restatement of the reference serial CPU path" % el}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "maxwell_ion_256^3", "grid": [n, n, n], "box_L": L,
+                           "gamma": 50.0, "kappa": 2.0, "closure": "maxwell", "tau_model": "ichimaru",
+                           "transport": "yukawa_fit", "dt": dt, "precision": "fp32 fields, fp64 sums",
+                           "parallelism": "replicas" if world > 1 else "single",
+                           "l2": "inputs larger than L2 (working set ~GBs)"},
+                "roofline": roof,
+                "step_roofline": {"bytes_per_cell_step": STEP_BYTES_FP32,
+                                  "achieved_GBps": STEP_BYTES_FP32 * value / world / 1e9,
+                                  "frac": STEP_BYTES_FP32 * value / world / 1e9 / peak},
+                "kernels": kernels,
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(gpu_launches),
+                "clocks": ck}
+        line.update(extra)
+        print(json.dumps(line), flush=True)
+    m32.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdio>
 #include <complex>
 #include <cstring>
 #include <memory>
@@ -351,6 +352,34 @@ int hydft_gpu_kernel(const hydft_gpu *h, double k, double *kk)
 {
     if (!h || !kk) return HYDFT_ERR_BAD_ARG;
     *kk = h->mh.kernel(k);
+    return HYDFT_OK;
+}
+
+int hydft_gpu_profile(hydft_gpu *h, int nsteps, int max_kernels, char *names, int names_len, double *total_ms,
+                      double *bytes_per_launch, int64_t *launches, int *nkernels)
+{
+    if (!h || nsteps < 1 || max_kernels < 1 || !names || names_len < 1) return HYDFT_ERR_BAD_ARG;
+    cudaSetDevice(h->device);
+    double t, dt;
+    int64_t stp;
+    h->s->get_time(&t, &dt, &stp);
+    if (!(dt > 0.0)) return fail(h, HYDFT_ERR_BAD_ARG, "dt is not set");
+    std::vector<KernelStat> ks;
+    int rc = h->s->profile(nsteps, ks);
+    if (rc) return wrap(h, rc);
+    std::string nm;
+    int k = 0;
+    for (auto &s : ks) {
+        if (k >= max_kernels) break;
+        if (k) nm += ",";
+        nm += s.name;
+        if (total_ms) total_ms[k] = s.ms;
+        if (bytes_per_launch) bytes_per_launch[k] = s.n ? s.bytes / (double)s.n : 0.0;
+        if (launches) launches[k] = s.n;
+        ++k;
+    }
+    std::snprintf(names, names_len, "%s", nm.c_str());
+    if (nkernels) *nkernels = k;
     return HYDFT_OK;
 }
 

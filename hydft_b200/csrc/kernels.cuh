@@ -275,6 +275,7 @@ struct Ctrl {
     long long step;
     StageScal st[3];
     double nkd_re, nkd_im;   // nhat at the drive mode, stage start
+    double pend_phi, pend_e; // relaxation factors of the pending stage
     unsigned status;
     int pending;             // Maxwell relaxation pending
 };
@@ -480,8 +481,8 @@ __global__ void combine_a_kernel(Grid g, Phys ph, int nm, CombineA<R> c, Ctrl *c
 {
     const size_t total = (size_t)g.nkzc * g.nkyc * g.pkx;
     const int pending = ctrl->pending;
-    const double phi = stage > 0 ? ctrl->st[stage - 1].phi : ctrl->st[2].phi;
-    const double ee = stage > 0 ? ctrl->st[stage - 1].e : ctrl->st[2].e;
+    const double phi = ctrl->pend_phi;
+    const double ee = ctrl->pend_e;
     for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
          idx += (size_t)gridDim.x * blockDim.x) {
         int kxc, kyc, kzc;
@@ -621,7 +622,11 @@ __global__ void combine_b_kernel(Grid g, Phys ph, int nm, CombineB<R> c, Ctrl *c
             }
         }
     }
-    if (!rhs_only && blockIdx.x == 0 && threadIdx.x == 0 && ph.evolve) ctrl->pending = 1;
+    if (!rhs_only && blockIdx.x == 0 && threadIdx.x == 0 && ph.evolve) {
+        ctrl->pending = 1;
+        ctrl->pend_phi = s.phi;
+        ctrl->pend_e = s.e;
+    }
 }
 
 // Completes a pending relaxation from u of the current state (combine U).
@@ -636,7 +641,7 @@ template <typename R>
 __global__ void combine_u_kernel(Grid g, Phys ph, int nm, CombineU<R> c, Ctrl *ctrl)
 {
     const size_t total = (size_t)g.nkzc * g.nkyc * g.pkx;
-    const double phi = ctrl->st[2].phi, ee = ctrl->st[2].e;
+    const double phi = ctrl->pend_phi, ee = ctrl->pend_e;
     for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
          idx += (size_t)gridDim.x * blockDim.x) {
         int kxc, kyc, kzc;
@@ -663,7 +668,6 @@ __global__ void combine_u_kernel(Grid g, Phys ph, int nm, CombineU<R> c, Ctrl *c
             c.P[q][idx] = p0[q] - R(phi) * (p0[q] - po) + R(ee) * (c.P[q][idx] - po);
         }
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) ctrl->pending = 0;
 }
 
 // Per-step scalars: stage times, drive amplitude and phase, relaxation factors.

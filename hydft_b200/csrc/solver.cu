@@ -200,6 +200,50 @@ public:
     cudaGraphExec_t gexec = nullptr;
     int xrb_a = 1, xrb_b = 1, xrb_io = 1;
     int smem_optin = 0;
+    bool host_pending = false;   // a Maxwell relaxation waits for u of the new state
+
+    // per-kernel CUDA-event timing (profile mode, uncaptured steps only)
+    struct KStat {
+        std::string name;
+        double ms = 0.0, bytes = 0.0;
+        int64_t n = 0;
+    };
+    std::vector<KStat> kstats;
+    struct EvRec {
+        int k;
+        cudaEvent_t a, b;
+    };
+    std::vector<EvRec> evrecs;
+    bool profiling = false;
+
+    template <class F>
+    void launch(const char *name, double bytes, F &&f)
+    {
+        cudaEvent_t a = nullptr, b = nullptr;
+        if (profiling) {
+            cudaEventCreate(&a);
+            cudaEventCreate(&b);
+            cudaEventRecord(a, st);
+        }
+        f();
+        launches++;
+        if (profiling) {
+            cudaEventRecord(b, st);
+            int k = -1;
+            for (size_t i = 0; i < kstats.size(); ++i)
+                if (kstats[i].name == name) k = (int)i;
+            if (k < 0) {
+                kstats.push_back(KStat());
+                kstats.back().name = name;
+                k = (int)kstats.size() - 1;
+            }
+            kstats[k].bytes += bytes;
+            kstats[k].n += 1;
+            evrecs.push_back({k, a, b});
+        }
+    }
+
+    double cb() const { return 2.0 * sizeof(R); }   // bytes of one complex value
 
     int precision_bits() const override { return sizeof(R) * 8; }
     void set_ext_omega(double w) override
@@ -393,8 +437,8 @@ public:
         }
         const int ntx = (g.nkxc + TX - 1) / TX;
         const size_t smz = sizeof(cplx<R>) * (2 * (size_t)g.nz * TX + g.nz);
-        zinv_kernel<R, TX><<<dim3(ntx, g.nkyc, nf), 256, smz, st>>>(g, a, twz);
-        launches++;
+        launch("zinv", nf * cb() * g.nkxc * g.nkyc * (double)(g.nkzc + g.nz),
+               [&] { zinv_kernel<R, TX><<<dim3(ntx, g.nkyc, nf), 256, smz, st>>>(g, a, twz); });
         if (g.ny > 1) {
             PassArgs<R> b;
             b.nf = nf;
@@ -404,8 +448,8 @@ public:
                 b.op[f] = OP_ID;
             }
             const size_t smy = sizeof(cplx<R>) * (2 * (size_t)g.ny * TX + g.ny);
-            yinv_kernel<R, TX><<<dim3(ntx, g.nz, nf), 256, smy, st>>>(g, b, twy);
-            launches++;
+            launch("yinv", nf * cb() * g.nkxc * g.nz * (double)(g.nkyc + g.ny),
+                   [&] { yinv_kernel<R, TX><<<dim3(ntx, g.nz, nf), 256, smy, st>>>(g, b, twy); });
         }
     }
 
@@ -423,8 +467,8 @@ public:
                 b.op[f] = OP_ID;
             }
             const size_t smy = sizeof(cplx<R>) * (2 * (size_t)g.ny * TX + g.ny);
-            yfwd_kernel<R, TX><<<dim3(ntx, g.nz, nf), 256, smy, st>>>(g, b, twy);
-            launches++;
+            launch("yfwd", nf * cb() * g.nkxc * g.nz * (double)(g.nkyc + g.ny),
+                   [&] { yfwd_kernel<R, TX><<<dim3(ntx, g.nz, nf), 256, smy, st>>>(g, b, twy); });
             src = zi;
         }
         PassArgs<R> a;
@@ -436,12 +480,12 @@ public:
         }
         const size_t smz = sizeof(cplx<R>) * (2 * (size_t)g.nz * TX + g.nz);
         const R norm = R(1.0 / ((double)g.nx * g.ny * g.nz));
-        zfwd_kernel<R, TX><<<dim3(ntx, g.nkyc, nf), 256, smz, st>>>(g, a, twz, norm);
-        launches++;
+        launch("zfwd", nf * cb() * g.nkxc * g.nkyc * (double)(g.nkzc + g.nz),
+               [&] { zfwd_kernel<R, TX><<<dim3(ntx, g.nkyc, nf), 256, smz, st>>>(g, a, twz, norm); });
     }
 
     template <class PW>
-    void xpass(int nin, int nout, const PW &pw, int rb)
+    void xpass(int nin, int nout, const PW &pw, int rb, const char *name = "xpass", int nreal = 0)
     {
         XArgs<R> a;
         a.nin = nin;
@@ -450,8 +494,8 @@ public:
         for (int f = 0; f < nout; ++f) a.out[f] = xo + (size_t)f * ysize;
         const int nrows = g.ny * g.nz;
         const size_t sm = xpass_smem<R>(g.nx, rb, nin, nout);
-        xpass_kernel<R, PW><<<(nrows + rb - 1) / rb, 256, sm, st>>>(g, a, twx, pw, rb);
-        launches++;
+        const double bytes = cb() * g.nkxc * (double)nrows * (nin + nout) + sizeof(R) * (double)ncell * nreal;
+        launch(name, bytes, [&] { xpass_kernel<R, PW><<<(nrows + rb - 1) / rb, 256, sm, st>>>(g, a, twx, pw, rb); });
     }
 
     int combine_grid() const
@@ -482,7 +526,7 @@ public:
         pw.ncell = ncell;
         pw.status = &ctrl->status;
         const int nout = nm + nm * (nm + 1) / 2 + 1;
-        xpass(nf, nout, pw, xrb_a);
+        xpass(nf, nout, pw, xrb_a, "xpass_a", write_u ? 1 + nm : 1);
         forward(nout, OA);
         CombineA<R> c;
         c.N = N;
@@ -494,8 +538,10 @@ public:
         c.Klin = Klin;
         c.MU = MU;
         for (int d = 0; d < 3; ++d) c.Q[d] = Q[d];
-        combine_a_kernel<R><<<combine_grid(), 256, 0, st>>>(g, ph, nm, c, ctrl, stage);
-        launches++;
+        const double ncomp = (double)g.nkxc * g.nkyc * g.nkzc;
+        const int nrw = 2 + nm + nm * (nm + 1) / 2 + 1 + nm + (ph.evolve ? 24 : 0);
+        launch("combine_a", ncomp * (cb() * nrw + sizeof(R)),
+               [&] { combine_a_kernel<R><<<combine_grid(), 256, 0, st>>>(g, ph, nm, c, ctrl, stage); });
     }
 
     void phase_b(int stage, bool rhs_only)
@@ -519,7 +565,7 @@ public:
         pw.ctrl = ctrl;
         pw.stage = stage;
         const int nout = nm + (ph.evolve ? 6 : 0);
-        xpass(nf, nout, pw, xrb_b);
+        xpass(nf, nout, pw, xrb_b, "xpass_b", ph.evolve ? 1 + nm : 1);
         forward(nout, OB);
         CombineB<R> c;
         c.N = N; c.RN = RN; c.oN = HN;
@@ -532,16 +578,20 @@ public:
             c.P[q] = P[q]; c.RP[q] = RP[q]; c.oP[q] = HP[q];
             c.V[q] = OB[ph.evolve ? nm + q : 0];
         }
-        combine_b_kernel<R><<<combine_grid(), 256, 0, st>>>(g, ph, nm, c, ctrl, stage, rhs_only ? 1 : 0);
-        launches++;
+        const double ncomp = (double)g.nkxc * g.nkyc * g.nkzc;
+        const int nrw = 2 + 5 * nm + 2 + (ph.evolve ? 30 : 0);
+        launch("combine_b", ncomp * cb() * nrw, [&] {
+            combine_b_kernel<R><<<combine_grid(), 256, 0, st>>>(g, ph, nm, c, ctrl, stage, rhs_only ? 1 : 0);
+        });
     }
 
     void begin_step()
     {
         const double omega = S.ext_kind == 2 ? S.ext_omega : 0.0;
-        begin_step_kernel<<<1, 32, 0, st>>>(ctrl, ph.evolve ? ph.tau : 0.0, S.ext_td, S.ext_amp, omega,
-                                            S.ext_ramp);
-        launches++;
+        launch("step_ctrl", 0.0, [&] {
+            begin_step_kernel<<<1, 32, 0, st>>>(ctrl, ph.evolve ? ph.tau : 0.0, S.ext_td, S.ext_amp, omega,
+                                                S.ext_ramp);
+        });
     }
 
     void one_step()
@@ -551,8 +601,7 @@ public:
             phase_a(s, ph.evolve != 0);
             phase_b(s, false);
         }
-        end_step_kernel<<<1, 32, 0, st>>>(ctrl);
-        launches++;
+        launch("step_ctrl", 0.0, [&] { end_step_kernel<<<1, 32, 0, st>>>(ctrl); });
     }
 
     // Maxwell: complete the last stage's relaxation from u of the new state
@@ -570,13 +619,61 @@ public:
         pw.nm = nm;
         pw.nhat = N;
         pw.status = &ctrl->status;
-        xpass(nf, nm, pw, xrb_io);
+        xpass(nf, nm, pw, xrb_io, "xpass_u");
         forward(nm, OA);
         CombineU<R> c;
         for (int q = 0; q < 6; ++q) { c.P[q] = P[q]; c.P0[q] = P0[q]; }
         for (int d = 0; d < 3; ++d) c.U[d] = OA[std::min(d, nm - 1)];
-        combine_u_kernel<R><<<combine_grid(), 256, 0, st>>>(g, ph, nm, c, ctrl);
-        launches++;
+        const double ncomp = (double)g.nkxc * g.nkyc * g.nkzc;
+        launch("combine_u", ncomp * cb() * (nm + 18),
+               [&] { combine_u_kernel<R><<<combine_grid(), 256, 0, st>>>(g, ph, nm, c, ctrl); });
+        cudaMemsetAsync(&ctrl->pending, 0, sizeof(int), st);
+    }
+
+    void finish_if_pending()
+    {
+        if (host_pending) finish();
+        host_pending = false;
+    }
+
+    int profile(int nsteps, std::vector<KernelStat> &out) override
+    {
+        std::vector<KStat> ks;
+        int rc = profile_k(nsteps, ks);
+        out.clear();
+        for (auto &k : ks) {
+            KernelStat o;
+            o.name = k.name;
+            o.ms = k.ms;
+            o.bytes = k.bytes;
+            o.n = k.n;
+            out.push_back(o);
+        }
+        return rc;
+    }
+
+    // Runs nsteps uncaptured steps with an event pair around every launch.
+    int profile_k(int nsteps, std::vector<KStat> &out)
+    {
+        CK(cudaStreamSynchronize(st));
+        kstats.clear();
+        evrecs.clear();
+        profiling = true;
+        for (int i = 0; i < nsteps; ++i) one_step();
+        host_pending = ph.evolve != 0;
+        profiling = false;
+        CK(cudaStreamSynchronize(st));
+        for (auto &e : evrecs) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e.a, e.b);
+            kstats[e.k].ms += ms;
+            cudaEventDestroy(e.a);
+            cudaEventDestroy(e.b);
+        }
+        evrecs.clear();
+        out = kstats;
+        CK(cudaGetLastError());
+        return check_status();
     }
 
     int check_status()
@@ -615,13 +712,14 @@ public:
             CK(cudaGraphLaunch(gexec, st));
             launches += step_launches;
         }
-        finish();
+        host_pending = ph.evolve != 0;
         CK(cudaGetLastError());
         return check_status();
     }
 
     int rhs(double t, double *dn, double *dmom, double *dpi) override
     {
+        finish_if_pending();
         // t only enters through the external force: set the stage scalars of
         // stage 0 at time t
         double t0, dt0;
@@ -732,12 +830,14 @@ public:
             if (int rc = from_real(6, sp, dp)) return rc;
         }
         CK(cudaMemsetAsync(&ctrl->pending, 0, sizeof(int), st));
+        host_pending = false;
         CK(cudaStreamSynchronize(st));
         return 0;
     }
 
     int get_state(double *n, double *mom, double *pi) override
     {
+        finish_if_pending();
         double nmean = 0.0;
         {
             cplx<R> h0;

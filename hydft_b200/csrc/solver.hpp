@@ -33,6 +33,13 @@ struct SolverSetup {
     std::vector<double> gauss_f;      // gaussian external force (3 real fields), optional
 };
 
+struct KernelStat {
+    std::string name;
+    double ms = 0.0;      // total device time of the launches (CUDA events)
+    double bytes = 0.0;   // total algorithmic bytes of the launches
+    int64_t n = 0;        // launches
+};
+
 class SolverBase {
 public:
     virtual ~SolverBase() {}
@@ -51,6 +58,8 @@ public:
     // drive frequency of the external potential (model_t%ext%omega); the
     // captured step graph is rebuilt on the next advance
     virtual void set_ext_omega(double w) = 0;
+    // nsteps uncaptured steps with CUDA events around every launch
+    virtual int profile(int nsteps, std::vector<KernelStat> &out) = 0;
     // the host-side setup constants in use
     virtual const SolverSetup &setup() const = 0;
     int64_t launches = 0;

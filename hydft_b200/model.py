@@ -105,6 +105,7 @@ def lib():
         L.hydft_gpu_set_scalar.argtypes = [_P, C.c_char_p, _D]
         L.hydft_gpu_get_structure.argtypes = [_P, C.POINTER(_I), _P, _P]
         L.hydft_gpu_kernel.argtypes = [_P, _D, C.POINTER(_D)]
+        L.hydft_gpu_profile.argtypes = [_P, _I, _I, C.c_char_p, _I, _P, _P, _P, C.POINTER(_I)]
         L.hydft_gpu_stream.restype = _P
         L.hydft_gpu_stream.argtypes = [_P]
         L.hydft_gpu_launch_count.restype = C.c_int64
@@ -302,6 +303,25 @@ class Model:
 
     def launch_count(self):
         return lib().hydft_gpu_launch_count(self.h)
+
+    def stream_ptr(self):
+        return lib().hydft_gpu_stream(self.h)
+
+    def profile(self, nsteps=1):
+        """Per-kernel CUDA-event timing of nsteps uncaptured steps:
+        {name: (total_ms, bytes_per_launch, launches)}."""
+        mk = 32
+        names = C.create_string_buffer(1024)
+        ms = np.zeros(mk)
+        by = np.zeros(mk)
+        nl = np.zeros(mk, dtype=np.int64)
+        nk = _I()
+        self._check(lib().hydft_gpu_profile(self.h, int(nsteps), mk, names, 1024, _ptr(ms), _ptr(by),
+                                            _ptr(nl), C.byref(nk)))
+        out = {}
+        for i, nmx in enumerate(names.value.decode().split(",")[: nk.value]):
+            out[nmx] = (float(ms[i]), float(by[i]), int(nl[i]))
+        return out
 
 
 def hnc_solve(potential, gamma, kappa, lam, n0, nr, rmax, tol, mix, maxiter, device=0):

@@ -186,6 +186,18 @@ void *hydft_gpu_stream(const hydft_gpu *h);
 /* Kernel launches made by the library since creation (for accounting). */
 int64_t hydft_gpu_launch_count(const hydft_gpu *h);
 
+/*
+ * Timing of the step's kernels: runs nsteps uncaptured RK3 steps with a
+ * CUDA event pair on the launching stream around every kernel, and reports
+ * per kernel class (names comma-separated into `names`): total device time
+ * in ms, algorithmic bytes per launch (each input read once, each output
+ * written once) and the number of launches.  The state advances by nsteps.
+ * No counterpart in the reference (it only times the run loop with
+ * cpu_time, src/hydft.f90:39-55).
+ */
+int hydft_gpu_profile(hydft_gpu *h, int nsteps, int max_kernels, char *names, int names_len,
+                      double *total_ms, double *bytes_per_launch, int64_t *launches, int *nkernels);
+
 /* ------------------------------------------------- setup on the device */
 
 /*
