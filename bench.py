@@ -198,6 +198,9 @@ def main():
     ap.add_argument("--ref-n", type=int, default=64)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-plain leg")
+    ap.add_argument("--quick", action="store_true",
+                    help="setup, warm-up and the timed steps only (for profiler captures)")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -220,7 +223,7 @@ def main():
     n = args.n
     L = 64.0
     st = structure_for_workload(hg, dev)
-    m32 = hg.Model(workload_params(hg, n, "fp32"), structure=st, device=dev)
+    m32 = hg.Model(workload_params(hg, n, args.precision), structure=st, device=dev)
     n0 = m32.scalar("n0")
     nin = initial_density(n, L, n0)
     zeros3 = np.zeros((3, n, n, n))
@@ -261,6 +264,14 @@ def main():
     cells = float(n) ** 3
     value = cells * args.steps * world / (ms_max * 1e-3)
     ms_step = ms_max / args.steps
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({"quick": True, "grid": n, "precision": args.precision, "value": value,
+                              "ms_per_step": ms_step, "gpu_launches": int(gpu_launches)}), flush=True)
+        m32.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
 
     # per-kernel device time of 2 uncaptured steps, CUDA events on the stream
     prof = m32.profile(2)

@@ -362,7 +362,7 @@ struct PWA {
 };
 
 // --------------------------------------------------------- phase B functor
-// inputs:  0..nm-1 d mu/dx_d, [Pi evolved: nm + c*nm + d  d Pi_c/dx_d]
+// inputs:  0..nm-1 d mu/dx_d, [Pi evolved: nm + 2((c/2) nm + d) + c%2  d Pi_c/dx_d]
 // outputs: 0..nm-1 n (dmu/dx_i - F_ext,i), [6 x  -u.grad Pi_c]
 template <typename R>
 struct PWB {
@@ -394,9 +394,11 @@ struct PWB {
         if (ph.evolve) {
             R u[3];
             for (int d = 0; d < nm; ++d) u[d] = u_real[d * ncell + q];
+            // input order: for component pairs (c, c+1), c even, and d < nm,
+            // the pair (d Pi_c/dx_d, d Pi_{c+1}/dx_d)
             for (int c = 0; c < 6; ++c) {
                 R acc = R(0);
-                for (int d = 0; d < nm; ++d) acc -= u[d] * Fin[(nm + c * nm + d) * stride];
+                for (int d = 0; d < nm; ++d) acc -= u[d] * Fin[(nm + 2 * ((c / 2) * nm + d) + (c % 2)) * stride];
                 Fout[(nm + c) * stride] = acc;
             }
         }
@@ -671,7 +673,7 @@ __global__ void combine_u_kernel(Grid g, Phys ph, int nm, CombineU<R> c, Ctrl *c
 }
 
 // Per-step scalars: stage times, drive amplitude and phase, relaxation factors.
-__global__ void begin_step_kernel(Ctrl *ctrl, double tau, int ext_td, double amp0, double omega,
+static __global__ void begin_step_kernel(Ctrl *ctrl, double tau, int ext_td, double amp0, double omega,
                                   double ramp)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -704,7 +706,7 @@ __global__ void begin_step_kernel(Ctrl *ctrl, double tau, int ext_td, double amp
     }
 }
 
-__global__ void end_step_kernel(Ctrl *ctrl)
+static __global__ void end_step_kernel(Ctrl *ctrl)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     ctrl->t = ctrl->t + ctrl->dt;

@@ -1,0 +1,465 @@
+// Transform passes built on the register FFT (regfft.cuh) for axis lengths
+// with a register plan (32, 48, 64, 96, 128, 192, 256).  Same data layouts
+// and semantics as the generic passes in kernels.cuh; these move each value
+// through shared memory once per transform instead of once per radix pass.
+//
+// y/z passes: TX consecutive kx columns on the fastest thread index (coalesced
+// 128-byte rows), T threads per column, G rows of the other axis per block.
+// x passes: T threads per row of x, blockDim/T rows per block; the phase A
+// and B physics runs in registers in block layout between the c2r and the
+// r2c, streamed over pairs of output fields.
+#pragma once
+
+#include "kernels.cuh"
+#include "regfft.cuh"
+
+namespace hydft {
+
+__device__ __forceinline__ int fft_signed(int n, int L) { return n <= L / 2 ? n : n - L; }
+
+// ------------------------------------------------------------ y/z passes
+template <typename R, int T, int E, int TX, int G>
+__global__ void __launch_bounds__(TX * T * G) zinv_fast(Grid g, PassArgs<R> a, const cplx<R> *twz)
+{
+    constexpr int L = T * E;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
+    cplx<R> *xb = tw + L;
+    const int tid = threadIdx.x, c = tid % TX, t = (tid / TX) % T, gi = tid / (TX * T);
+    const int x = blockIdx.x * TX + c, kyc = blockIdx.y * G + gi, f = blockIdx.z;
+    const bool valid = x < g.nkxc && kyc < g.nkyc;
+    const cplx<R> *__restrict__ in = a.in[f];
+    cplx<R> *__restrict__ out = a.out[f];
+    const int op = a.op[f];
+    for (int i = tid; i < L; i += blockDim.x) tw[i] = twz[i];
+    const int my = valid ? signed_idx(kyc, g.My) : 0;
+    const R kx = R(x * g.kx0), ky = R(my * g.ky0);
+    cplx<R> v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int mz = fft_signed(t + T * e, L);
+        cplx<R> z = {R(0), R(0)};
+        if (valid && mz >= -g.Mz && mz <= g.Mz) {
+            const int kzc = mz >= 0 ? mz : mz + g.nkzc;
+            z = in[((size_t)kzc * g.nkyc + kyc) * g.pkx + x];
+            const R kz = R(mz * g.kz0);
+            switch (op) {
+            case OP_ZK0: if (x == 0 && my == 0 && mz == 0) z = cplx<R>{R(0), R(0)}; break;
+            case OP_IKX: z = ik_times(kx, z); break;
+            case OP_IKY: z = ik_times(ky, z); break;
+            case OP_IKZ: z = ik_times(kz, z); break;
+            case OP_NK2: z = R(-(kx * kx + ky * ky + kz * kz)) * z; break;
+            default: break;
+            }
+        }
+        v[e] = z;
+    }
+    __syncthreads();
+    stride_to_block<T, E, +1>(v, t, xb + gi * (L + L / T) * TX + c, TX, tw);
+    if (valid) {
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+            const int z = block_pos<T, E>(t, r);
+            out[((size_t)z * g.nkyc + kyc) * g.pkx + x] = v[r];
+        }
+    }
+}
+
+template <typename R, int T, int E, int TX, int G>
+__global__ void __launch_bounds__(TX * T * G) yinv_fast(Grid g, PassArgs<R> a, const cplx<R> *twy)
+{
+    constexpr int L = T * E;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
+    cplx<R> *xb = tw + L;
+    const int tid = threadIdx.x, c = tid % TX, t = (tid / TX) % T, gi = tid / (TX * T);
+    const int x = blockIdx.x * TX + c, z = blockIdx.y * G + gi, f = blockIdx.z;
+    const bool valid = x < g.nkxc && z < g.nz;
+    const cplx<R> *__restrict__ in = a.in[f];
+    cplx<R> *__restrict__ out = a.out[f];
+    for (int i = tid; i < L; i += blockDim.x) tw[i] = twy[i];
+    cplx<R> v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int my = fft_signed(t + T * e, L);
+        cplx<R> val = {R(0), R(0)};
+        if (valid && my >= -g.My && my <= g.My) {
+            const int kyc = my >= 0 ? my : my + g.nkyc;
+            val = in[((size_t)z * g.nkyc + kyc) * g.pkx + x];
+        }
+        v[e] = val;
+    }
+    __syncthreads();
+    stride_to_block<T, E, +1>(v, t, xb + gi * (L + L / T) * TX + c, TX, tw);
+    if (valid) {
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+            const int y = block_pos<T, E>(t, r);
+            out[((size_t)z * g.ny + y) * g.pkx + x] = v[r];
+        }
+    }
+}
+
+template <typename R, int T, int E, int TX, int G>
+__global__ void __launch_bounds__(TX * T * G) yfwd_fast(Grid g, PassArgs<R> a, const cplx<R> *twy)
+{
+    constexpr int L = T * E;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
+    cplx<R> *xb = tw + L;
+    const int tid = threadIdx.x, c = tid % TX, t = (tid / TX) % T, gi = tid / (TX * T);
+    const int x = blockIdx.x * TX + c, z = blockIdx.y * G + gi, f = blockIdx.z;
+    const bool valid = x < g.nkxc && z < g.nz;
+    const cplx<R> *__restrict__ in = a.in[f];
+    cplx<R> *__restrict__ out = a.out[f];
+    for (int i = tid; i < L; i += blockDim.x) tw[i] = twy[i];
+    cplx<R> v[E];
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+        const int y = block_pos<T, E>(t, r);
+        v[r] = valid ? in[((size_t)z * g.ny + y) * g.pkx + x] : cplx<R>{R(0), R(0)};
+    }
+    __syncthreads();
+    block_to_stride<T, E, -1>(v, t, xb + gi * (L + L / T) * TX + c, TX, tw);
+    if (valid) {
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            const int my = fft_signed(t + T * m, L);
+            if (my >= -g.My && my <= g.My) {
+                const int kyc = my >= 0 ? my : my + g.nkyc;
+                out[((size_t)z * g.nkyc + kyc) * g.pkx + x] = v[m];
+            }
+        }
+    }
+}
+
+template <typename R, int T, int E, int TX, int G>
+__global__ void __launch_bounds__(TX * T * G) zfwd_fast(Grid g, PassArgs<R> a, const cplx<R> *twz, R norm)
+{
+    constexpr int L = T * E;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
+    cplx<R> *xb = tw + L;
+    const int tid = threadIdx.x, c = tid % TX, t = (tid / TX) % T, gi = tid / (TX * T);
+    const int x = blockIdx.x * TX + c, kyc = blockIdx.y * G + gi, f = blockIdx.z;
+    const bool valid = x < g.nkxc && kyc < g.nkyc;
+    const cplx<R> *__restrict__ in = a.in[f];
+    cplx<R> *__restrict__ out = a.out[f];
+    for (int i = tid; i < L; i += blockDim.x) tw[i] = twz[i];
+    cplx<R> v[E];
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+        const int z = block_pos<T, E>(t, r);
+        v[r] = valid ? in[((size_t)z * g.nkyc + kyc) * g.pkx + x] : cplx<R>{R(0), R(0)};
+    }
+    __syncthreads();
+    block_to_stride<T, E, -1>(v, t, xb + gi * (L + L / T) * TX + c, TX, tw);
+    if (valid) {
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            const int mz = fft_signed(t + T * m, L);
+            if (mz >= -g.Mz && mz <= g.Mz) {
+                const int kzc = mz >= 0 ? mz : mz + g.nkzc;
+                out[((size_t)kzc * g.nkyc + kyc) * g.pkx + x] = norm * v[m];
+            }
+        }
+    }
+}
+
+// smem bytes of a y/z fast pass
+template <typename R>
+inline size_t yz_fast_smem(int L, int T, int TX, int G)
+{
+    return sizeof(cplx<R>) * ((size_t)L + (size_t)G * (L + L / T) * TX);
+}
+
+// --------------------------------------------------------------- x passes
+// row exchange buffer stride (pad so rows sharing a half-warp use other banks)
+template <int T, int E>
+__host__ __device__ constexpr int xrow_stride() { return T * E + E + 1; }
+
+// c2r input of a pair of half spectra (kx <= Mx, XF/YI layout) in stride
+// layout, then inverse FFT to block layout: v[r] = a(x) + i b(x) at
+// x = block_pos(t, r).  inb may be null (b = 0).
+template <typename R, int T, int E>
+__device__ __forceinline__ void x_c2r_pair(cplx<R> (&v)[E], const cplx<R> *__restrict__ ina,
+                                           const cplx<R> *__restrict__ inb, int row, bool rowok, int t,
+                                           const Grid &g, cplx<R> *xrow, const cplx<R> *tw)
+{
+    constexpr int L = T * E;
+    const int Mx = g.Mx;
+    const size_t base = (size_t)row * g.pkx;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int k = t + T * e;
+        cplx<R> Z = {R(0), R(0)};
+        if (rowok) {
+            if (k <= Mx) {
+                cplx<R> va = ina[base + k];
+                cplx<R> vb = inb ? inb[base + k] : cplx<R>{R(0), R(0)};
+                if (k == 0) { va.y = R(0); vb.y = R(0); }
+                Z = cplx<R>{va.x - vb.y, va.y + vb.x};
+            } else if (k >= L - Mx) {
+                const int kk = L - k;
+                cplx<R> va = ina[base + kk];
+                cplx<R> vb = inb ? inb[base + kk] : cplx<R>{R(0), R(0)};
+                Z = cplx<R>{va.x + vb.y, -va.y + vb.x};
+            }
+        }
+        v[e] = Z;
+    }
+    stride_to_block<T, E, +1>(v, t, xrow, 1, tw);
+}
+
+// r2c of z = a + i b given in block layout; writes the half spectra of a
+// and b for kx <= Mx (outb may be null)
+template <typename R, int T, int E>
+__device__ __forceinline__ void x_r2c_pair(cplx<R> (&v)[E], cplx<R> *__restrict__ outa, cplx<R> *__restrict__ outb,
+                                           int row, bool rowok, int t, const Grid &g, cplx<R> *xrow,
+                                           const cplx<R> *tw)
+{
+    constexpr int L = T * E;
+    block_to_stride<T, E, -1>(v, t, xrow, 1, tw);
+#pragma unroll
+    for (int m = 0; m < E; ++m) xrow[xidx<T>(t + T * m)] = v[m];
+    __syncthreads();
+    const size_t base = (size_t)row * g.pkx;
+    if (rowok) {
+        for (int k = t; k <= g.Mx; k += T) {
+            const cplx<R> zk = xrow[xidx<T>(k)];
+            const cplx<R> zm = conj(xrow[xidx<T>(k == 0 ? 0 : L - k)]);
+            outa[base + k] = R(0.5) * (zk + zm);
+            if (outb) outb[base + k] = mul_i<-1>(R(0.5) * (zk - zm));
+        }
+    }
+    __syncthreads();
+}
+
+template <typename R>
+struct XFastArgs {
+    const cplx<R> *in[MAXF];
+    cplx<R> *out[MAXF];
+    int nin, nout;
+};
+
+// packed (i <= j) flux index -> (i, j) for three components
+__host__ __device__ constexpr int flux_i3(int f) { return f < 3 ? 0 : (f < 5 ? 1 : 2); }
+__host__ __device__ constexpr int flux_j3(int f) { return f < 3 ? f : (f < 5 ? f - 2 : 2); }
+
+// Phase A (3-D): inputs dn, m_0..m_2 [, dn/dx_0..2, lap n]; outputs u_d,
+// the fluxes m_i u_j (i <= j) and mu_local (UONLY: u_d only).  Input pairs
+// and mu_local are kept in per-thread shared-memory slots (block layout);
+// each output pair is then computed, transformed and written in turn.
+template <typename R, int T, int E, int NM, bool GRAD, bool UONLY>
+__global__ void __launch_bounds__(256) xa_fast(Grid g, XFastArgs<R> a, const cplx<R> *twx, PWA<R> pw)
+{
+    static_assert(NM == 3, "fast x pass is for 3-D grids");
+    constexpr int L = T * E;
+    constexpr int NIN = 1 + NM + (GRAD ? NM + 1 : 0);
+    constexpr int NP = (NIN + 1) / 2;
+    constexpr int NF = NM * (NM + 1) / 2;
+    constexpr int NOUT = UONLY ? NM : NM + NF + 1;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
+    cplx<R> *xbuf = tw + L;
+    const int nt = blockDim.x, rb = nt / T;
+    cplx<R> *slots = xbuf + rb * xrow_stride<T, E>();
+    R *muslot = reinterpret_cast<R *>(slots + NP * E * nt);
+    const int tid = threadIdx.x, t = tid % T, rr = tid / T;
+    const int row = blockIdx.x * rb + rr;
+    const bool rowok = row < g.ny * g.nz;
+    cplx<R> *xrow = xbuf + rr * xrow_stride<T, E>();
+    for (int i = tid; i < L; i += nt) tw[i] = twx[i];
+    __syncthreads();
+#pragma unroll 1
+    for (int p = 0; p < NP; ++p) {
+        cplx<R> v[E];
+        x_c2r_pair<R, T, E>(v, a.in[2 * p], 2 * p + 1 < NIN ? a.in[2 * p + 1] : nullptr, row, rowok, t, g, xrow, tw);
+#pragma unroll
+        for (int r = 0; r < E; ++r) slots[(p * E + r) * nt + tid] = v[r];
+    }
+    auto input = [&](int f, int r) -> R {
+        const cplx<R> s = slots[((f / 2) * E + r) * nt + tid];
+        return (f & 1) ? s.y : s.x;
+    };
+    const double nref = (double)pw.nhat[0].x;
+    const size_t rowbase = (size_t)row * g.nx;
+    // density check, real-space dn and u for phase B, local chemical potential
+#pragma unroll 1
+    for (int r = 0; r < E; ++r) {
+        const int xx = block_pos<T, E>(t, r);
+        const R dn = input(0, r);
+        const double n = nref + (double)dn;
+        if (rowok) {
+            if (!(n > 0.0)) atomicOr(pw.status, isfinite(n) ? ST_NONPOS : ST_NONFINITE);
+            if (pw.dn_real) pw.dn_real[rowbase + xx] = dn;
+            if (pw.u_real) {
+                const R inv_mn = R(1.0 / (pw.ph.mass * n));
+                for (int d = 0; d < NM; ++d) pw.u_real[d * pw.ncell + rowbase + xx] = input(1 + d, r) * inv_mn;
+            }
+        }
+        if (!UONLY) {
+            double mu = 0.0, alpha = 0.0;
+            bool have_alpha = false;
+            for (int tt = 0; tt < pw.ph.nterms_local; ++tt) {
+                const int id = pw.ph.term_order[tt];
+                if (id == 1) {
+                    mu += log1p((double)dn / nref) * pw.ph.inv_beta;
+                } else {
+                    if (!have_alpha) {
+                        bool ok = true;
+                        alpha = fd::alpha_from_ip12(pw.fdtab, n / pw.ph.cn, &ok);
+                        if (!ok && rowok) atomicOr(pw.status, ST_NONPOS);
+                        have_alpha = true;
+                    }
+                    if (id == 2) {
+                        mu += (alpha - pw.ph.alpha_ref) * pw.ph.inv_beta;
+                    } else if (GRAD) {
+                        const double xi = fd::xi(pw.fdtab, alpha);
+                        const double dxidn = fd::dxi(pw.fdtab, alpha) / (0.5 * pw.ph.cn * fd::im12(pw.fdtab, alpha));
+                        double g2 = 0.0;
+                        for (int d = 0; d < NM; ++d) {
+                            const double gd = (double)input(1 + NM + d, r);
+                            g2 += gd * gd;
+                        }
+                        const double lapn = (double)input(1 + 2 * NM, r);
+                        mu -= pw.ph.cg * (dxidn * g2 + 2.0 * xi * lapn);
+                    }
+                }
+            }
+            muslot[r * nt + tid] = R(mu);
+        }
+    }
+    // output pairs
+#pragma unroll
+    for (int q = 0; 2 * q < NOUT; ++q) {
+        cplx<R> v[E];
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+            const R inv_mn = R(1.0 / (pw.ph.mass * (nref + (double)input(0, r))));
+            R val[2] = {R(0), R(0)};
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int o = 2 * q + h;
+                if (o < NM) val[h] = input(1 + o, r) * inv_mn;
+                else if (o < NM + NF) val[h] = input(1 + flux_i3(o - NM), r) * (input(1 + flux_j3(o - NM), r) * inv_mn);
+                else if (o < NOUT) val[h] = muslot[r * nt + tid];
+            }
+            v[r] = cplx<R>{val[0], val[1]};
+        }
+        x_r2c_pair<R, T, E>(v, a.out[2 * q], 2 * q + 1 < NOUT ? a.out[2 * q + 1] : nullptr, row, rowok, t, g, xrow, tw);
+    }
+}
+
+// Phase B: inputs [d mu/dx_0 ..], then for each Pi component pair (c, c+1)
+// and d < NM the pair (d Pi_c/dx_d, d Pi_{c+1}/dx_d); outputs
+// n (d mu/dx_i - F_i) and, when Pi evolves, -u.grad Pi_c.
+template <typename R, int T, int E, int NM, bool EVOLVE>
+__global__ void __launch_bounds__(256) xb_fast(Grid g, XFastArgs<R> a, const cplx<R> *twx, PWB<R> pw)
+{
+    constexpr int L = T * E;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
+    cplx<R> *xbuf = tw + L;
+    const int nt = blockDim.x, rb = nt / T;
+    const int tid = threadIdx.x, t = tid % T, rr = tid / T;
+    const int row = blockIdx.x * rb + rr;
+    const bool rowok = row < g.ny * g.nz;
+    cplx<R> *xrow = xbuf + rr * xrow_stride<T, E>();
+    for (int i = tid; i < L; i += nt) tw[i] = twx[i];
+    __syncthreads();
+    const double nref = (double)pw.nhat[0].x;
+    const size_t rowbase = (size_t)row * g.nx;
+    const int y = rowok ? row % g.ny : 0, z = rowok ? row / g.ny : 0;
+    // n (dmu - F): pairs of components
+#pragma unroll
+    for (int q = 0; 2 * q < NM; ++q) {
+        const int i0 = 2 * q, i1 = 2 * q + 1;
+        cplx<R> v[E];
+        x_c2r_pair<R, T, E>(v, a.in[i0], i1 < NM ? a.in[i1] : nullptr, row, rowok, t, g, xrow, tw);
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+            const int xx = block_pos<T, E>(t, r);
+            const R n = rowok ? R(nref + (double)pw.dn_real[rowbase + xx]) : R(0);
+            R f0 = R(0), f1 = R(0);
+            if (pw.ph.ext_active) {
+                const StageScal &s = pw.ctrl->st[pw.stage];
+                cplx<double> e = pw.ex[xx] * pw.ey[y];
+                e = e * pw.ez[z];
+                e = e * cplx<double>{s.ewr, s.ewi};
+                const double sf = s.amp * e.y;
+                f0 = R(sf * pw.ph.ext_k[i0]);
+                if (i1 < NM) f1 = R(sf * pw.ph.ext_k[i1]);
+            }
+            v[r] = cplx<R>{n * (v[r].x - f0), n * (v[r].y - f1)};
+        }
+        x_r2c_pair<R, T, E>(v, a.out[i0], i1 < NM ? a.out[i1] : nullptr, row, rowok, t, g, xrow, tw);
+    }
+    if (EVOLVE) {
+        // -u.grad Pi for component pairs (0,1), (2,3), (4,5)
+#pragma unroll 1
+        for (int cp = 0; cp < 3; ++cp) {
+            cplx<R> acc[E];
+#pragma unroll
+            for (int r = 0; r < E; ++r) acc[r] = cplx<R>{R(0), R(0)};
+#pragma unroll
+            for (int d = 0; d < NM; ++d) {
+                const int f = NM + 2 * (cp * NM + d);
+                cplx<R> v[E];
+                x_c2r_pair<R, T, E>(v, a.in[f], a.in[f + 1], row, rowok, t, g, xrow, tw);
+#pragma unroll
+                for (int r = 0; r < E; ++r) {
+                    const int xx = block_pos<T, E>(t, r);
+                    const R u = rowok ? pw.u_real[d * pw.ncell + rowbase + xx] : R(0);
+                    acc[r] = acc[r] - u * v[r];
+                }
+            }
+            x_r2c_pair<R, T, E>(acc, a.out[NM + 2 * cp], a.out[NM + 2 * cp + 1], row, rowok, t, g, xrow, tw);
+        }
+    }
+}
+
+// Real-space I/O: half spectra -> real fields (TOREAL) or back.
+template <typename R, int T, int E, bool TOREAL>
+__global__ void __launch_bounds__(256) xio_fast(Grid g, XFastArgs<R> a, const cplx<R> *twx, PWToReal<R> dst,
+                                                PWFromReal<R> src)
+{
+    constexpr int L = T * E;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
+    cplx<R> *xbuf = tw + L;
+    const int nt = blockDim.x, rb = nt / T;
+    const int tid = threadIdx.x, t = tid % T, rr = tid / T;
+    const int row = blockIdx.x * rb + rr;
+    const bool rowok = row < g.ny * g.nz;
+    cplx<R> *xrow = xbuf + rr * xrow_stride<T, E>();
+    for (int i = tid; i < L; i += nt) tw[i] = twx[i];
+    __syncthreads();
+    const size_t rowbase = (size_t)row * g.nx;
+    const int nf = TOREAL ? a.nin : a.nout;
+    for (int p = 0; 2 * p < nf; ++p) {
+        const int fa = 2 * p, fb = 2 * p + 1;
+        cplx<R> v[E];
+        if (TOREAL) {
+            x_c2r_pair<R, T, E>(v, a.in[fa], fb < nf ? a.in[fb] : nullptr, row, rowok, t, g, xrow, tw);
+            if (rowok) {
+#pragma unroll
+                for (int r = 0; r < E; ++r) {
+                    const int xx = block_pos<T, E>(t, r);
+                    dst.dst[fa][rowbase + xx] = v[r].x;
+                    if (fb < nf) dst.dst[fb][rowbase + xx] = v[r].y;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int r = 0; r < E; ++r) {
+                const int xx = block_pos<T, E>(t, r);
+                v[r] = rowok ? cplx<R>{src.src[fa][rowbase + xx], fb < nf ? src.src[fb][rowbase + xx] : R(0)}
+                             : cplx<R>{R(0), R(0)};
+            }
+            x_r2c_pair<R, T, E>(v, a.out[fa], fb < nf ? a.out[fb] : nullptr, row, rowok, t, g, xrow, tw);
+        }
+    }
+}
+
+}  // namespace hydft

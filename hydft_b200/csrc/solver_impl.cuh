@@ -1,4 +1,4 @@
-// Device solver for one simulation: buffers, transform pipelines and the
+// Device solver for one simulation (included once per precision): buffers, transform pipelines and the
 // per-stage kernel sequence of the RK3 step.
 //
 // Per RK stage (model.f90:192-223 restated on a spectral-resident state):
@@ -20,7 +20,10 @@
 #include <vector>
 
 #include "kernels.cuh"
+#include "passes_fast.cuh"
 #include "solver.hpp"
+
+#include <type_traits>
 
 namespace hydft {
 
@@ -170,6 +173,28 @@ static void make_twiddles(int L, std::vector<cplx<R>> &tw)
     }
 }
 
+// Calls f(integral_constant<T>, integral_constant<E>) for an axis length
+// with a register FFT plan; returns false otherwise.
+template <class F>
+static bool with_plan(int L, F &&f)
+{
+    using std::integral_constant;
+    switch (L) {
+    case 32: f(integral_constant<int, 4>{}, integral_constant<int, 8>{}); return true;
+    case 48: f(integral_constant<int, 4>{}, integral_constant<int, 12>{}); return true;
+    case 64: f(integral_constant<int, 8>{}, integral_constant<int, 8>{}); return true;
+    case 96: f(integral_constant<int, 4>{}, integral_constant<int, 24>{}); return true;
+    case 128: f(integral_constant<int, 8>{}, integral_constant<int, 16>{}); return true;
+    case 256: f(integral_constant<int, 16>{}, integral_constant<int, 16>{}); return true;
+    default: return false;
+    }
+}
+
+static bool has_plan(int L)
+{
+    return L == 32 || L == 48 || L == 64 || L == 96 || L == 128 || L == 256;
+}
+
 template <typename R>
 class Solver : public SolverBase {
 public:
@@ -201,6 +226,7 @@ public:
     int xrb_a = 1, xrb_b = 1, xrb_io = 1;
     int smem_optin = 0;
     bool host_pending = false;   // a Maxwell relaxation waits for u of the new state
+    bool fast_x = false;         // x passes on the register FFT (3-D grids, planned nx)
 
     // per-kernel CUDA-event timing (profile mode, uncaptured steps only)
     struct KStat {
@@ -394,6 +420,23 @@ public:
         xrb_b = pick_rb(ninB, noutB);
         xrb_io = pick_rb(10, 10);
         if (int rc = set_smem_attrs()) return rc;
+        {
+            RegTw rt;
+            const double pi = 3.14159265358979323846264338327950288;
+            auto fill = [&](double (*w)[2], int N) {
+                for (int j = 0; j < N; ++j) {
+                    w[j][0] = std::cos(2.0 * pi * j / N);
+                    w[j][1] = -std::sin(2.0 * pi * j / N);
+                }
+            };
+            fill(rt.w6, 6);
+            fill(rt.w12, 12);
+            fill(rt.w16, 16);
+            fill(rt.w24, 24);
+            fill(rt.w32, 32);
+            CK(cudaMemcpyToSymbol(c_regtw, &rt, sizeof(rt)));
+        }
+        fast_x = has_plan(g.nx) && nm == 3;
         // uniform initial state n = n0, mom = 0, Pi = 0 (species.f90:155-169)
         set_k0_kernel<R><<<1, 32, 0, st>>>(N, s.n0);
         launches++;
@@ -426,6 +469,17 @@ public:
     // ------------------------------------------------------------ pipelines
     // inverse transform of nf spectral fields (with load-time operators) into
     // YI buffers 0..nf-1
+    static constexpr int YZ_TX = sizeof(R) == 4 ? 16 : 8;
+    static constexpr int YZ_NT = sizeof(R) == 4 ? 256 : 128;
+
+    template <class K>
+    void set_smem(K k, size_t bytes)
+    {
+        if (bytes > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    }
+
+    // inverse transform of nf spectral fields (with load-time operators) into
+    // YI buffers 0..nf-1
     void inverse(int nf, const cplx<R> *const *src, const int *ops)
     {
         PassArgs<R> a;
@@ -435,10 +489,21 @@ public:
             a.out[f] = zi + (size_t)f * zsize;
             a.op[f] = ops[f];
         }
-        const int ntx = (g.nkxc + TX - 1) / TX;
-        const size_t smz = sizeof(cplx<R>) * (2 * (size_t)g.nz * TX + g.nz);
-        launch("zinv", nf * cb() * g.nkxc * g.nkyc * (double)(g.nkzc + g.nz),
-               [&] { zinv_kernel<R, TX><<<dim3(ntx, g.nkyc, nf), 256, smz, st>>>(g, a, twz); });
+        const double zbytes = nf * cb() * g.nkxc * g.nkyc * (double)(g.nkzc + g.nz);
+        const bool zf = with_plan(g.nz, [&](auto Tc, auto Ec) {
+            constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value, TX = YZ_TX;
+            constexpr int G = YZ_NT / (TX * T) > 0 ? YZ_NT / (TX * T) : 1;
+            const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
+            auto k = zinv_fast<R, T, E, TX, G>;
+            set_smem(k, sm);
+            const dim3 grid((g.nkxc + TX - 1) / TX, (g.nkyc + G - 1) / G, nf);
+            launch("zinv", zbytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, a, twz); });
+        });
+        if (!zf) {
+            const int ntx = (g.nkxc + TX - 1) / TX;
+            const size_t smz = sizeof(cplx<R>) * (2 * (size_t)g.nz * TX + g.nz);
+            launch("zinv", zbytes, [&] { zinv_kernel<R, TX><<<dim3(ntx, g.nkyc, nf), 256, smz, st>>>(g, a, twz); });
+        }
         if (g.ny > 1) {
             PassArgs<R> b;
             b.nf = nf;
@@ -447,9 +512,21 @@ public:
                 b.out[f] = yi + (size_t)f * ysize;
                 b.op[f] = OP_ID;
             }
-            const size_t smy = sizeof(cplx<R>) * (2 * (size_t)g.ny * TX + g.ny);
-            launch("yinv", nf * cb() * g.nkxc * g.nz * (double)(g.nkyc + g.ny),
-                   [&] { yinv_kernel<R, TX><<<dim3(ntx, g.nz, nf), 256, smy, st>>>(g, b, twy); });
+            const double ybytes = nf * cb() * g.nkxc * g.nz * (double)(g.nkyc + g.ny);
+            const bool yf = with_plan(g.ny, [&](auto Tc, auto Ec) {
+                constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value, TX = YZ_TX;
+                constexpr int G = YZ_NT / (TX * T) > 0 ? YZ_NT / (TX * T) : 1;
+                const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
+                auto k = yinv_fast<R, T, E, TX, G>;
+                set_smem(k, sm);
+                const dim3 grid((g.nkxc + TX - 1) / TX, (g.nz + G - 1) / G, nf);
+                launch("yinv", ybytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, b, twy); });
+            });
+            if (!yf) {
+                const int ntx = (g.nkxc + TX - 1) / TX;
+                const size_t smy = sizeof(cplx<R>) * (2 * (size_t)g.ny * TX + g.ny);
+                launch("yinv", ybytes, [&] { yinv_kernel<R, TX><<<dim3(ntx, g.nz, nf), 256, smy, st>>>(g, b, twy); });
+            }
         }
     }
 
@@ -466,9 +543,20 @@ public:
                 b.out[f] = zi + (size_t)f * zsize;
                 b.op[f] = OP_ID;
             }
-            const size_t smy = sizeof(cplx<R>) * (2 * (size_t)g.ny * TX + g.ny);
-            launch("yfwd", nf * cb() * g.nkxc * g.nz * (double)(g.nkyc + g.ny),
-                   [&] { yfwd_kernel<R, TX><<<dim3(ntx, g.nz, nf), 256, smy, st>>>(g, b, twy); });
+            const double ybytes = nf * cb() * g.nkxc * g.nz * (double)(g.nkyc + g.ny);
+            const bool yf = with_plan(g.ny, [&](auto Tc, auto Ec) {
+                constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value, TX = YZ_TX;
+                constexpr int G = YZ_NT / (TX * T) > 0 ? YZ_NT / (TX * T) : 1;
+                const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
+                auto k = yfwd_fast<R, T, E, TX, G>;
+                set_smem(k, sm);
+                const dim3 grid((g.nkxc + TX - 1) / TX, (g.nz + G - 1) / G, nf);
+                launch("yfwd", ybytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, b, twy); });
+            });
+            if (!yf) {
+                const size_t smy = sizeof(cplx<R>) * (2 * (size_t)g.ny * TX + g.ny);
+                launch("yfwd", ybytes, [&] { yfwd_kernel<R, TX><<<dim3(ntx, g.nz, nf), 256, smy, st>>>(g, b, twy); });
+            }
             src = zi;
         }
         PassArgs<R> a;
@@ -478,10 +566,107 @@ public:
             a.out[f] = dst[f];
             a.op[f] = OP_ID;
         }
-        const size_t smz = sizeof(cplx<R>) * (2 * (size_t)g.nz * TX + g.nz);
         const R norm = R(1.0 / ((double)g.nx * g.ny * g.nz));
-        launch("zfwd", nf * cb() * g.nkxc * g.nkyc * (double)(g.nkzc + g.nz),
-               [&] { zfwd_kernel<R, TX><<<dim3(ntx, g.nkyc, nf), 256, smz, st>>>(g, a, twz, norm); });
+        const double zbytes = nf * cb() * g.nkxc * g.nkyc * (double)(g.nkzc + g.nz);
+        const bool zf = with_plan(g.nz, [&](auto Tc, auto Ec) {
+            constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value, TX = YZ_TX;
+            constexpr int G = YZ_NT / (TX * T) > 0 ? YZ_NT / (TX * T) : 1;
+            const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
+            auto k = zfwd_fast<R, T, E, TX, G>;
+            set_smem(k, sm);
+            const dim3 grid((g.nkxc + TX - 1) / TX, (g.nkyc + G - 1) / G, nf);
+            launch("zfwd", zbytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, a, twz, norm); });
+        });
+        if (!zf) {
+            const size_t smz = sizeof(cplx<R>) * (2 * (size_t)g.nz * TX + g.nz);
+            launch("zfwd", zbytes, [&] { zfwd_kernel<R, TX><<<dim3(ntx, g.nkyc, nf), 256, smz, st>>>(g, a, twz, norm); });
+        }
+    }
+
+    // threads of a fast x pass: the largest multiple of T up to 256 whose
+    // shared memory stays within ~110 KB
+    template <int T, int E>
+    int x_threads(int np_slots, size_t &smem) const
+    {
+        int nt = 256;
+        for (;;) {
+            smem = sizeof(cplx<R>) * ((size_t)T * E + (size_t)(nt / T) * xrow_stride<T, E>() + (size_t)np_slots * E * nt) +
+                   (np_slots ? sizeof(R) * (size_t)E * nt : 0);
+            if (smem <= 110 * 1024 || nt <= T) break;
+            nt /= 2;
+        }
+        return nt;
+    }
+
+    XFastArgs<R> xargs(int nin, int nout) const
+    {
+        XFastArgs<R> a;
+        a.nin = nin;
+        a.nout = nout;
+        for (int f = 0; f < nin; ++f) a.in[f] = yi + (size_t)f * ysize;
+        for (int f = 0; f < nout; ++f) a.out[f] = xo + (size_t)f * ysize;
+        return a;
+    }
+
+    double xbytes(int nin, int nout, int nreal) const
+    {
+        return cb() * g.nkxc * (double)g.ny * g.nz * (nin + nout) + sizeof(R) * (double)ncell * nreal;
+    }
+
+    // fast phase-A x pass (3-D); uonly: u only (relaxation finish)
+    void xa_launch(int nin, int nout, const PWA<R> &pw, bool grad, bool uonly, const char *name, int nreal)
+    {
+        const XFastArgs<R> a = xargs(nin, nout);
+        const int nrows = g.ny * g.nz;
+        with_plan(g.nx, [&](auto Tc, auto Ec) {
+            constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value;
+            auto go = [&](auto k, int np) {
+                size_t sm;
+                const int nt = x_threads<T, E>(np, sm);
+                set_smem(k, sm);
+                const int rb = nt / T;
+                launch(name, xbytes(nin, nout, nreal), [&] { k<<<(nrows + rb - 1) / rb, nt, sm, st>>>(g, a, twx, pw); });
+            };
+            if (uonly) go(xa_fast<R, T, E, 3, false, true>, 2);
+            else if (grad) go(xa_fast<R, T, E, 3, true, false>, 4);
+            else go(xa_fast<R, T, E, 3, false, false>, 2);
+        });
+    }
+
+    void xb_launch(int nin, int nout, const PWB<R> &pw, int nreal)
+    {
+        const XFastArgs<R> a = xargs(nin, nout);
+        const int nrows = g.ny * g.nz;
+        with_plan(g.nx, [&](auto Tc, auto Ec) {
+            constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value;
+            auto go = [&](auto k) {
+                size_t sm;
+                const int nt = x_threads<T, E>(0, sm);
+                set_smem(k, sm);
+                const int rb = nt / T;
+                launch("xpass_b", xbytes(nin, nout, nreal), [&] { k<<<(nrows + rb - 1) / rb, nt, sm, st>>>(g, a, twx, pw); });
+            };
+            if (ph.evolve) go(xb_fast<R, T, E, 3, true>);
+            else go(xb_fast<R, T, E, 3, false>);
+        });
+    }
+
+    void xio_launch(int nin, int nout, const PWToReal<R> &dst, const PWFromReal<R> &src, const char *name)
+    {
+        const XFastArgs<R> a = xargs(nin, nout);
+        const int nrows = g.ny * g.nz;
+        with_plan(g.nx, [&](auto Tc, auto Ec) {
+            constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value;
+            auto go = [&](auto k) {
+                size_t sm;
+                const int nt = x_threads<T, E>(0, sm);
+                set_smem(k, sm);
+                const int rb = nt / T;
+                launch(name, xbytes(nin, nout, nin + nout), [&] { k<<<(nrows + rb - 1) / rb, nt, sm, st>>>(g, a, twx, dst, src); });
+            };
+            if (nin > 0) go(xio_fast<R, T, E, true>);
+            else go(xio_fast<R, T, E, false>);
+        });
     }
 
     template <class PW>
@@ -526,7 +711,8 @@ public:
         pw.ncell = ncell;
         pw.status = &ctrl->status;
         const int nout = nm + nm * (nm + 1) / 2 + 1;
-        xpass(nf, nout, pw, xrb_a, "xpass_a", write_u ? 1 + nm : 1);
+        if (fast_x) xa_launch(nf, nout, pw, ph.has_grad != 0, false, "xpass_a", write_u ? 1 + nm : 1);
+        else xpass(nf, nout, pw, xrb_a, "xpass_a", write_u ? 1 + nm : 1);
         forward(nout, OA);
         CombineA<R> c;
         c.N = N;
@@ -551,8 +737,9 @@ public:
         int nf = 0;
         for (int d = 0; d < nm; ++d) { src[nf] = MU; ops[nf++] = OP_IKX + d; }
         if (ph.evolve)
-            for (int c = 0; c < 6; ++c)
-                for (int d = 0; d < nm; ++d) { src[nf] = P[c]; ops[nf++] = OP_IKX + d; }
+            for (int cp = 0; cp < 3; ++cp)
+                for (int d = 0; d < nm; ++d)
+                    for (int h = 0; h < 2; ++h) { src[nf] = P[2 * cp + h]; ops[nf++] = OP_IKX + d; }
         inverse(nf, src, ops);
         PWB<R> pw;
         pw.ph = ph;
@@ -565,7 +752,8 @@ public:
         pw.ctrl = ctrl;
         pw.stage = stage;
         const int nout = nm + (ph.evolve ? 6 : 0);
-        xpass(nf, nout, pw, xrb_b, "xpass_b", ph.evolve ? 1 + nm : 1);
+        if (fast_x) xb_launch(nf, nout, pw, ph.evolve ? 1 + nm : 1);
+        else xpass(nf, nout, pw, xrb_b, "xpass_b", ph.evolve ? 1 + nm : 1);
         forward(nout, OB);
         CombineB<R> c;
         c.N = N; c.RN = RN; c.oN = HN;
@@ -614,12 +802,25 @@ public:
         src[nf] = N; ops[nf++] = OP_ZK0;
         for (int d = 0; d < nm; ++d) { src[nf] = M[d]; ops[nf++] = OP_ID; }
         inverse(nf, src, ops);
-        PWU<R> pw;
-        pw.ph = ph;
-        pw.nm = nm;
-        pw.nhat = N;
-        pw.status = &ctrl->status;
-        xpass(nf, nm, pw, xrb_io, "xpass_u");
+        if (fast_x) {
+            PWA<R> pa;
+            pa.ph = ph;
+            pa.nm = nm;
+            pa.nhat = N;
+            pa.fdtab = fdtab;
+            pa.dn_real = nullptr;
+            pa.u_real = nullptr;
+            pa.ncell = ncell;
+            pa.status = &ctrl->status;
+            xa_launch(nf, nm, pa, false, true, "xpass_u", 0);
+        } else {
+            PWU<R> pw;
+            pw.ph = ph;
+            pw.nm = nm;
+            pw.nhat = N;
+            pw.status = &ctrl->status;
+            xpass(nf, nm, pw, xrb_io, "xpass_u");
+        }
         forward(nm, OA);
         CombineU<R> c;
         for (int q = 0; q < 6; ++q) { c.P[q] = P[q]; c.P0[q] = P0[q]; }
@@ -759,9 +960,21 @@ public:
         PWToReal<R> pw;
         for (int f = 0; f < MAXF; ++f) pw.dst[f] = f < nf ? dst[f] : nullptr;
         pw.ncell = ncell;
-        xpass(nf, 0, pw, xrb_io);
+        x_toreal(nf, pw);
         CK(cudaGetLastError());
         return 0;
+    }
+
+    void x_toreal(int nf, const PWToReal<R> &pw)
+    {
+        if (fast_x) {
+            PWFromReal<R> none;
+            for (int f = 0; f < MAXF; ++f) none.src[f] = nullptr;
+            none.nf = 0;
+            xio_launch(nf, 0, pw, none, "xpass_io");
+        } else {
+            xpass(nf, 0, pw, xrb_io, "xpass_io");
+        }
     }
 
     // real-space device arrays -> compact fields (masked to the band)
@@ -770,7 +983,14 @@ public:
         PWFromReal<R> pw;
         for (int f = 0; f < MAXF; ++f) pw.src[f] = f < nf ? src[f] : nullptr;
         pw.nf = nf;
-        xpass(0, nf, pw, xrb_io);
+        if (fast_x) {
+            PWToReal<R> none;
+            for (int f = 0; f < MAXF; ++f) none.dst[f] = nullptr;
+            none.ncell = ncell;
+            xio_launch(0, nf, none, pw, "xpass_io");
+        } else {
+            xpass(0, nf, pw, xrb_io, "xpass_io");
+        }
         forward(nf, const_cast<cplx<R> *const *>(dst));
         CK(cudaGetLastError());
         return 0;
@@ -859,7 +1079,7 @@ public:
             PWToReal<R> pw;
             for (int f = 0; f < MAXF; ++f) pw.dst[f] = f < nf ? dsts[f] : nullptr;
             pw.ncell = ncell;
-            xpass(nf, 0, pw, xrb_io);
+            x_toreal(nf, pw);
         }
         if (n) if (int rc = down(n, io_real, 1, nmean)) return rc;
         if (mom) if (int rc = down(mom, io_real + ncell, 3, 0.0)) return rc;
@@ -883,7 +1103,7 @@ public:
         pw.dst[0] = io_real;
         for (int d = 0; d < nm; ++d) pw.dst[1 + d] = io_real + (1 + d) * ncell;
         pw.ncell = ncell;
-        xpass(1 + nm, 0, pw, xrb_io);
+        x_toreal(1 + nm, pw);
         reduce_fields_kernel<R><<<red_blocks, 256, 0, st>>>(io_real, io_real + ncell, ncell, nm, N,
                                                             ph.inv_mass, rpart);
         reduce_final_kernel<R><<<1, 32, 0, st>>>(rpart, red_blocks, rout);
@@ -947,25 +1167,17 @@ public:
     }
 };
 
-SolverBase *make_solver(const SolverSetup &s, int precision, int device, std::string &err)
+// One precision per translation unit (solver_f32.cu / solver_f64.cu).
+SolverBase *HYDFT_MAKE_FN(const SolverSetup &s, int device, std::string &err)
 {
-    SolverBase *r = nullptr;
-    int rc = 0;
-    if (precision == 32) {
-        auto *p = new Solver<float>();
-        rc = p->init(s, device);
-        r = p;
-    } else {
-        auto *p = new Solver<double>();
-        rc = p->init(s, device);
-        r = p;
-    }
-    if (rc) {
-        err = r->err;
-        delete r;
+    auto *p = new Solver<HYDFT_REAL>();
+    if (int rc = p->init(s, device)) {
+        (void)rc;
+        err = p->err;
+        delete p;
         return nullptr;
     }
-    return r;
+    return p;
 }
 
 }  // namespace hydft

@@ -102,6 +102,16 @@ CASES = {
     "ion_nodealias_mode": dict(ION, nx=24, ny=6, nz=6, lx=20.0, ly=5.0, lz=5.0, dealias=False,
                                vext="mode", vext_amplitude=1e-3, vext_mode=(1, 1, 1), eta=0.4,
                                transport="constant"),
+    # sizes with register-FFT plans on every axis (32, 48, 64, 96, 256)
+    "fast_ion_maxwell_32x48x64": dict(ION, nx=32, ny=48, nz=64, lx=16.0, ly=24.0, lz=32.0,
+                                      closure="maxwell", tau_model="constant", tau=1.5),
+    "fast_electron_driven_64x96x32": dict(ELEC, nx=64, ny=96, nz=32, lx=20.0, ly=30.0, lz=10.0,
+                                          closure="newtonian", vext="driven", vext_amplitude=1e-3,
+                                          vext_mode=(3, -1, 1), vext_omega=1.1, vext_ramp=0.0),
+    "fast_ion_newtonian_256x8x8": dict(ION, nx=256, ny=8, nz=8, lx=64.0, ly=4.0, lz=4.0,
+                                       closure="newtonian"),
+    "fast_ion_maxwell_16x16x256": dict(ION, nx=16, ny=16, nz=256, lx=8.0, ly=8.0, lz=64.0,
+                                       closure="maxwell", tau_model="constant", tau=0.7),
 }
 
 
@@ -142,7 +152,8 @@ def test_advance_fp64(hg, orc, case):
         assert rel(g[2], o.pi) < TOL64, rel(g[2], o.pi)
 
 
-@pytest.mark.parametrize("case", ["ion_newtonian_3d", "ion_maxwell_3d", "electron_driven_3d"])
+@pytest.mark.parametrize("case", ["ion_newtonian_3d", "ion_maxwell_3d", "electron_driven_3d",
+                                  "fast_ion_maxwell_32x48x64", "fast_electron_driven_64x96x32"])
 def test_advance_fp32(hg, orc, case):
     m, o = pair(hg, orc, dt=0.02, gpu_precision="fp32", **CASES[case])
     n, mom, pi = seeded_state(m)
