@@ -374,6 +374,7 @@ struct PWB {
     const cplx<double> *ex, *ey, *ez;   // exp(i k_d x_d) per axis
     const Ctrl *ctrl;
     int stage;
+    unsigned *status;
 
     __device__ void operator()(const Grid &g, int row, int x, const R *Fin, R *Fout, int stride) const
     {

@@ -38,24 +38,38 @@ __global__ void __launch_bounds__(TX * T * G) zinv_fast(Grid g, PassArgs<R> a, c
 #pragma unroll
     for (int e = 0; e < E; ++e) {
         const int mz = fft_signed(t + T * e, L);
-        cplx<R> z = {R(0), R(0)};
-        if (valid && mz >= -g.Mz && mz <= g.Mz) {
-            const int kzc = mz >= 0 ? mz : mz + g.nkzc;
-            z = in[((size_t)kzc * g.nkyc + kyc) * g.pkx + x];
-            const R kz = R(mz * g.kz0);
-            switch (op) {
-            case OP_ZK0: if (x == 0 && my == 0 && mz == 0) z = cplx<R>{R(0), R(0)}; break;
-            case OP_IKX: z = ik_times(kx, z); break;
-            case OP_IKY: z = ik_times(ky, z); break;
-            case OP_IKZ: z = ik_times(kz, z); break;
-            case OP_NK2: z = R(-(kx * kx + ky * ky + kz * kz)) * z; break;
-            default: break;
-            }
+        const bool ok = valid && mz >= -g.Mz && mz <= g.Mz;
+        const int kzc = mz >= 0 ? mz : mz + g.nkzc;
+        v[e] = ok ? in[((size_t)kzc * g.nkyc + kyc) * g.pkx + x] : cplx<R>{R(0), R(0)};
+    }
+    // the operator is uniform over the block
+    switch (op) {
+    case OP_ZK0:
+        if (x == 0 && my == 0 && t == 0) v[0] = cplx<R>{R(0), R(0)};
+        break;
+    case OP_IKX:
+#pragma unroll
+        for (int e = 0; e < E; ++e) v[e] = ik_times(kx, v[e]);
+        break;
+    case OP_IKY:
+#pragma unroll
+        for (int e = 0; e < E; ++e) v[e] = ik_times(ky, v[e]);
+        break;
+    case OP_IKZ:
+#pragma unroll
+        for (int e = 0; e < E; ++e) v[e] = ik_times(R(fft_signed(t + T * e, L) * g.kz0), v[e]);
+        break;
+    case OP_NK2:
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const R kz = R(fft_signed(t + T * e, L) * g.kz0);
+            v[e] = R(-(kx * kx + ky * ky + kz * kz)) * v[e];
         }
-        v[e] = z;
+        break;
+    default: break;
     }
     __syncthreads();
-    stride_to_block<T, E, +1>(v, t, xb + gi * (L + L / T) * TX + c, TX, tw);
+    stride_to_block<T, E, +1, R, BarBlock, TX>(v, t, xb + gi * (L + L / T) * TX + c, tw);
     if (valid) {
 #pragma unroll
         for (int r = 0; r < E; ++r) {
@@ -90,7 +104,7 @@ __global__ void __launch_bounds__(TX * T * G) yinv_fast(Grid g, PassArgs<R> a, c
         v[e] = val;
     }
     __syncthreads();
-    stride_to_block<T, E, +1>(v, t, xb + gi * (L + L / T) * TX + c, TX, tw);
+    stride_to_block<T, E, +1, R, BarBlock, TX>(v, t, xb + gi * (L + L / T) * TX + c, tw);
     if (valid) {
 #pragma unroll
         for (int r = 0; r < E; ++r) {
@@ -120,7 +134,7 @@ __global__ void __launch_bounds__(TX * T * G) yfwd_fast(Grid g, PassArgs<R> a, c
         v[r] = valid ? in[((size_t)z * g.ny + y) * g.pkx + x] : cplx<R>{R(0), R(0)};
     }
     __syncthreads();
-    block_to_stride<T, E, -1>(v, t, xb + gi * (L + L / T) * TX + c, TX, tw);
+    block_to_stride<T, E, -1, R, BarBlock, TX>(v, t, xb + gi * (L + L / T) * TX + c, tw);
     if (valid) {
 #pragma unroll
         for (int m = 0; m < E; ++m) {
@@ -153,7 +167,7 @@ __global__ void __launch_bounds__(TX * T * G) zfwd_fast(Grid g, PassArgs<R> a, c
         v[r] = valid ? in[((size_t)z * g.nkyc + kyc) * g.pkx + x] : cplx<R>{R(0), R(0)};
     }
     __syncthreads();
-    block_to_stride<T, E, -1>(v, t, xb + gi * (L + L / T) * TX + c, TX, tw);
+    block_to_stride<T, E, -1, R, BarBlock, TX>(v, t, xb + gi * (L + L / T) * TX + c, tw);
     if (valid) {
 #pragma unroll
         for (int m = 0; m < E; ++m) {
@@ -174,9 +188,11 @@ inline size_t yz_fast_smem(int L, int T, int TX, int G)
 }
 
 // --------------------------------------------------------------- x passes
-// row exchange buffer stride (pad so rows sharing a half-warp use other banks)
+// row exchange buffer stride: the padded row (L + L/T elements) rounded up
+// to 16 elements, plus T when several rows share a half-warp, so that row r
+// starts at bank group r*T and the rows of a half-warp never collide
 template <int T, int E>
-__host__ __device__ constexpr int xrow_stride() { return T * E + E + 1; }
+__host__ __device__ constexpr int xrow_stride() { return (T * E + E + 15) / 16 * 16 + (T < 16 ? T : 0); }
 
 // c2r input of a pair of half spectra (kx <= Mx, XF/YI layout) in stride
 // layout, then inverse FFT to block layout: v[r] = a(x) + i b(x) at
@@ -208,7 +224,7 @@ __device__ __forceinline__ void x_c2r_pair(cplx<R> (&v)[E], const cplx<R> *__res
         }
         v[e] = Z;
     }
-    stride_to_block<T, E, +1>(v, t, xrow, 1, tw);
+    stride_to_block<T, E, +1, R, BarWarp, 1>(v, t, xrow, tw);
 }
 
 // r2c of z = a + i b given in block layout; writes the half spectra of a
@@ -219,10 +235,10 @@ __device__ __forceinline__ void x_r2c_pair(cplx<R> (&v)[E], cplx<R> *__restrict_
                                            const cplx<R> *tw)
 {
     constexpr int L = T * E;
-    block_to_stride<T, E, -1>(v, t, xrow, 1, tw);
+    block_to_stride<T, E, -1, R, BarWarp, 1>(v, t, xrow, tw);
 #pragma unroll
-    for (int m = 0; m < E; ++m) xrow[xidx<T>(t + T * m)] = v[m];
-    __syncthreads();
+    for (int m = 0; m < E; ++m) xrow[t + m * (T + 1)] = v[m];   // element t + T m
+    __syncwarp();
     const size_t base = (size_t)row * g.pkx;
     if (rowok) {
         for (int k = t; k <= g.Mx; k += T) {
@@ -232,7 +248,7 @@ __device__ __forceinline__ void x_r2c_pair(cplx<R> (&v)[E], cplx<R> *__restrict_
             if (outb) outb[base + k] = mul_i<-1>(R(0.5) * (zk - zm));
         }
     }
-    __syncthreads();
+    __syncwarp();
 }
 
 template <typename R>
@@ -250,8 +266,12 @@ __host__ __device__ constexpr int flux_j3(int f) { return f < 3 ? f : (f < 5 ? f
 // the fluxes m_i u_j (i <= j) and mu_local (UONLY: u_d only).  Input pairs
 // and mu_local are kept in per-thread shared-memory slots (block layout);
 // each output pair is then computed, transformed and written in turn.
+#ifndef HYDFT_XMINB
+#define HYDFT_XMINB 1
+#endif
+
 template <typename R, int T, int E, int NM, bool GRAD, bool UONLY>
-__global__ void __launch_bounds__(256) xa_fast(Grid g, XFastArgs<R> a, const cplx<R> *twx, PWA<R> pw)
+__global__ void __launch_bounds__(256, HYDFT_XMINB) xa_fast(Grid g, XFastArgs<R> a, const cplx<R> *twx, PWA<R> pw)
 {
     static_assert(NM == 3, "fast x pass is for 3-D grids");
     constexpr int L = T * E;
@@ -265,6 +285,7 @@ __global__ void __launch_bounds__(256) xa_fast(Grid g, XFastArgs<R> a, const cpl
     const int nt = blockDim.x, rb = nt / T;
     cplx<R> *slots = xbuf + rb * xrow_stride<T, E>();
     R *muslot = reinterpret_cast<R *>(slots + NP * E * nt);
+    R *invslot = muslot + E * nt;
     const int tid = threadIdx.x, t = tid % T, rr = tid / T;
     const int row = blockIdx.x * rb + rr;
     const bool rowok = row < g.ny * g.nz;
@@ -282,38 +303,47 @@ __global__ void __launch_bounds__(256) xa_fast(Grid g, XFastArgs<R> a, const cpl
         const cplx<R> s = slots[((f / 2) * E + r) * nt + tid];
         return (f & 1) ? s.y : s.x;
     };
-    const double nref = (double)pw.nhat[0].x;
+    // the mean density is exact in the k = 0 mode; deviations carry the
+    // signal, so n, 1/(m n) and ln(n/nref) are formed in the field precision
+    const R nref = pw.nhat[0].x;
+    const R inv_nref = R(1) / nref, inv_beta = R(pw.ph.inv_beta), mass = R(pw.ph.mass);
     const size_t rowbase = (size_t)row * g.nx;
-    // density check, real-space dn and u for phase B, local chemical potential
+    // density check, real-space dn and u for phase B, 1/(m n) and the local
+    // chemical potential into per-thread slots
 #pragma unroll 1
     for (int r = 0; r < E; ++r) {
         const int xx = block_pos<T, E>(t, r);
         const R dn = input(0, r);
-        const double n = nref + (double)dn;
+        const R n = nref + dn;
+        const R inv_mn = R(1) / (mass * n);
+        invslot[r * nt + tid] = inv_mn;
         if (rowok) {
-            if (!(n > 0.0)) atomicOr(pw.status, isfinite(n) ? ST_NONPOS : ST_NONFINITE);
+            if (!(n > R(0))) atomicOr(pw.status, isfinite(n) ? ST_NONPOS : ST_NONFINITE);
             if (pw.dn_real) pw.dn_real[rowbase + xx] = dn;
             if (pw.u_real) {
-                const R inv_mn = R(1.0 / (pw.ph.mass * n));
                 for (int d = 0; d < NM; ++d) pw.u_real[d * pw.ncell + rowbase + xx] = input(1 + d, r) * inv_mn;
             }
         }
         if (!UONLY) {
-            double mu = 0.0, alpha = 0.0;
-            bool have_alpha = false;
+            R mu = R(0);
+            double mu64 = 0.0, alpha = 0.0;
+            bool have_alpha = false, any64 = false;
             for (int tt = 0; tt < pw.ph.nterms_local; ++tt) {
                 const int id = pw.ph.term_order[tt];
                 if (id == 1) {
-                    mu += log1p((double)dn / nref) * pw.ph.inv_beta;
+                    mu += log1p(dn * inv_nref) * inv_beta;
                 } else {
+                    // alpha(n) by FP64 Newton on the Fermi-Dirac table
+                    const double n64 = (double)nref + (double)dn;
+                    any64 = true;
                     if (!have_alpha) {
                         bool ok = true;
-                        alpha = fd::alpha_from_ip12(pw.fdtab, n / pw.ph.cn, &ok);
+                        alpha = fd::alpha_from_ip12(pw.fdtab, n64 / pw.ph.cn, &ok);
                         if (!ok && rowok) atomicOr(pw.status, ST_NONPOS);
                         have_alpha = true;
                     }
                     if (id == 2) {
-                        mu += (alpha - pw.ph.alpha_ref) * pw.ph.inv_beta;
+                        mu64 += (alpha - pw.ph.alpha_ref) * pw.ph.inv_beta;
                     } else if (GRAD) {
                         const double xi = fd::xi(pw.fdtab, alpha);
                         const double dxidn = fd::dxi(pw.fdtab, alpha) / (0.5 * pw.ph.cn * fd::im12(pw.fdtab, alpha));
@@ -323,11 +353,11 @@ __global__ void __launch_bounds__(256) xa_fast(Grid g, XFastArgs<R> a, const cpl
                             g2 += gd * gd;
                         }
                         const double lapn = (double)input(1 + 2 * NM, r);
-                        mu -= pw.ph.cg * (dxidn * g2 + 2.0 * xi * lapn);
+                        mu64 -= pw.ph.cg * (dxidn * g2 + 2.0 * xi * lapn);
                     }
                 }
             }
-            muslot[r * nt + tid] = R(mu);
+            muslot[r * nt + tid] = any64 ? R((double)mu + mu64) : mu;
         }
     }
     // output pairs
@@ -336,7 +366,7 @@ __global__ void __launch_bounds__(256) xa_fast(Grid g, XFastArgs<R> a, const cpl
         cplx<R> v[E];
 #pragma unroll
         for (int r = 0; r < E; ++r) {
-            const R inv_mn = R(1.0 / (pw.ph.mass * (nref + (double)input(0, r))));
+            const R inv_mn = invslot[r * nt + tid];
             R val[2] = {R(0), R(0)};
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
@@ -355,7 +385,7 @@ __global__ void __launch_bounds__(256) xa_fast(Grid g, XFastArgs<R> a, const cpl
 // and d < NM the pair (d Pi_c/dx_d, d Pi_{c+1}/dx_d); outputs
 // n (d mu/dx_i - F_i) and, when Pi evolves, -u.grad Pi_c.
 template <typename R, int T, int E, int NM, bool EVOLVE>
-__global__ void __launch_bounds__(256) xb_fast(Grid g, XFastArgs<R> a, const cplx<R> *twx, PWB<R> pw)
+__global__ void __launch_bounds__(256, HYDFT_XMINB) xb_fast(Grid g, XFastArgs<R> a, const cplx<R> *twx, PWB<R> pw)
 {
     constexpr int L = T * E;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -368,7 +398,7 @@ __global__ void __launch_bounds__(256) xb_fast(Grid g, XFastArgs<R> a, const cpl
     cplx<R> *xrow = xbuf + rr * xrow_stride<T, E>();
     for (int i = tid; i < L; i += nt) tw[i] = twx[i];
     __syncthreads();
-    const double nref = (double)pw.nhat[0].x;
+    const R nref = pw.nhat[0].x;
     const size_t rowbase = (size_t)row * g.nx;
     const int y = rowok ? row % g.ny : 0, z = rowok ? row / g.ny : 0;
     // n (dmu - F): pairs of components
@@ -380,7 +410,7 @@ __global__ void __launch_bounds__(256) xb_fast(Grid g, XFastArgs<R> a, const cpl
 #pragma unroll
         for (int r = 0; r < E; ++r) {
             const int xx = block_pos<T, E>(t, r);
-            const R n = rowok ? R(nref + (double)pw.dn_real[rowbase + xx]) : R(0);
+            const R n = rowok ? nref + pw.dn_real[rowbase + xx] : R(0);
             R f0 = R(0), f1 = R(0);
             if (pw.ph.ext_active) {
                 const StageScal &s = pw.ctrl->st[pw.stage];

@@ -105,51 +105,61 @@ struct RegDFT<24, DIR, R> : RegDFTComp<8, 3, DIR, R> {};
 template <int DIR, typename R>
 struct RegDFT<32, DIR, R> : RegDFTComp<4, 8, DIR, R> {};
 
-// Shared-memory exchange buffer of one column: element e at sm[idx(e)*es],
-// with one pad slot every T elements so that the strided reads of the
-// exchange hit distinct banks.
+// Shared-memory exchange buffer of one column: element e at
+// sm[(e + e/T) * ES] (one pad slot every T elements, so that the strided
+// reads of the exchange hit distinct banks).  The index expressions below
+// are that formula with t < T and E % T == 0 folded in, so every access is
+// a per-thread base plus a compile-time offset.
 template <int T>
 __device__ __forceinline__ int xidx(int e) { return e + e / T; }
 
+// Barrier policies of the exchange: the whole block (a column's threads
+// span warps) or one warp (a column's threads are lanes of one warp).
+struct BarBlock {
+    static __device__ __forceinline__ void sync() { __syncthreads(); }
+};
+struct BarWarp {
+    static __device__ __forceinline__ void sync() { __syncwarp(); }
+};
+
 // x in stride layout (v[e] = x[t + T e]) -> X in block layout
 // (v[j*T + k1] = X[(t + T j) + E k1]).  `sm` is this column's exchange
-// buffer (element stride es), `tw` the W_L table.  Ends with a barrier of
-// the participating threads (bar = __syncthreads).
-template <int T, int E, int DIR, typename R>
-__device__ __forceinline__ void stride_to_block(cplx<R> (&v)[E], int t, cplx<R> *sm, int es,
+// buffer (element stride ES), `tw` the W_L table.
+template <int T, int E, int DIR, typename R, class BAR = BarBlock, int ES = 1>
+__device__ __forceinline__ void stride_to_block(cplx<R> (&v)[E], int t, cplx<R> *sm,
                                                 const cplx<R> *__restrict__ tw)
 {
-    constexpr int L = T * E;
     RegDFT<E, DIR, R>::run(v);
 #pragma unroll
     for (int k2 = 1; k2 < E; ++k2) {
-        cplx<R> w = tw[(t * k2) % L];
+        cplx<R> w = tw[t * k2];   // t*k2 < T*E = L
         if (DIR > 0) w.y = -w.y;
         v[k2] = v[k2] * w;
     }
+    cplx<R> *wp = sm + t * ES;
 #pragma unroll
-    for (int k2 = 0; k2 < E; ++k2) sm[xidx<T>(k2 * T + t) * es] = v[k2];
-    __syncthreads();
+    for (int k2 = 0; k2 < E; ++k2) wp[k2 * (T + 1) * ES] = v[k2];   // element k2*T + t
+    BAR::sync();
 #pragma unroll
     for (int j = 0; j < E / T; ++j) {
-        const int k2 = t + T * j;
+        const cplx<R> *rp = sm + (t + T * j) * (T + 1) * ES;         // element (t + T j)*T + n1
         cplx<R> u[T];
 #pragma unroll
-        for (int n1 = 0; n1 < T; ++n1) u[n1] = sm[xidx<T>(k2 * T + n1) * es];
+        for (int n1 = 0; n1 < T; ++n1) u[n1] = rp[n1 * ES];
         RegDFT<T, DIR, R>::run(u);
 #pragma unroll
         for (int k1 = 0; k1 < T; ++k1) v[j * T + k1] = u[k1];
     }
-    __syncthreads();
+    BAR::sync();
 }
 
 // z in block layout (v[j*T + k1] = z[(t + T j) + E k1]) -> X in stride
 // layout (v[m] = X[t + T m]).
-template <int T, int E, int DIR, typename R>
-__device__ __forceinline__ void block_to_stride(cplx<R> (&v)[E], int t, cplx<R> *sm, int es,
+template <int T, int E, int DIR, typename R, class BAR = BarBlock, int ES = 1>
+__device__ __forceinline__ void block_to_stride(cplx<R> (&v)[E], int t, cplx<R> *sm,
                                                 const cplx<R> *__restrict__ tw)
 {
-    constexpr int L = T * E;
+    constexpr int EP = E + E / T;   // padded length of E elements
 #pragma unroll
     for (int j = 0; j < E / T; ++j) {
         const int k2 = t + T * j;
@@ -157,18 +167,20 @@ __device__ __forceinline__ void block_to_stride(cplx<R> (&v)[E], int t, cplx<R> 
 #pragma unroll
         for (int k1 = 0; k1 < T; ++k1) u[k1] = v[j * T + k1];
         RegDFT<T, DIR, R>::run(u);
+        cplx<R> *wp = sm + (t + j * (T + 1)) * ES;                   // element m1*E + k2
 #pragma unroll
         for (int m1 = 0; m1 < T; ++m1) {
-            cplx<R> w = tw[(k2 * m1) % L];
+            cplx<R> w = tw[k2 * m1];   // k2*m1 < E*T = L
             if (DIR > 0) w.y = -w.y;
-            sm[xidx<T>(m1 * E + k2) * es] = m1 == 0 ? u[0] : u[m1] * w;
+            wp[m1 * EP * ES] = m1 == 0 ? u[0] : u[m1] * w;
         }
     }
-    __syncthreads();
+    BAR::sync();
+    const cplx<R> *rp = sm + t * EP * ES;                             // element t*E + k2
 #pragma unroll
-    for (int k2 = 0; k2 < E; ++k2) v[k2] = sm[xidx<T>(t * E + k2) * es];
+    for (int k2 = 0; k2 < E; ++k2) v[k2] = rp[(k2 + k2 / T) * ES];
     RegDFT<E, DIR, R>::run(v);
-    __syncthreads();
+    BAR::sync();
 }
 
 // position (index along the axis) of register r in block layout

@@ -16,12 +16,15 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "kernels.cuh"
 #include "passes_fast.cuh"
 #include "solver.hpp"
+#include "xpass_tma.cuh"
 
 #include <type_traits>
 
@@ -227,6 +230,8 @@ public:
     int smem_optin = 0;
     bool host_pending = false;   // a Maxwell relaxation waits for u of the new state
     bool fast_x = false;         // x passes on the register FFT (3-D grids, planned nx)
+    bool tma_x = false;          // persistent TMA-fed x passes (HYDFT_XPASS=tma); measured slower
+    int num_sms = 148;
 
     // per-kernel CUDA-event timing (profile mode, uncaptured steps only)
     struct KStat {
@@ -437,6 +442,11 @@ public:
             CK(cudaMemcpyToSymbol(c_regtw, &rt, sizeof(rt)));
         }
         fast_x = has_plan(g.nx) && nm == 3;
+        {
+            const char *ev = std::getenv("HYDFT_XPASS");
+            if (ev && std::string(ev) == "tma") tma_x = true;
+            CK(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
+        }
         // uniform initial state n = n0, mom = 0, Pi = 0 (species.f90:155-169)
         set_k0_kernel<R><<<1, 32, 0, st>>>(N, s.n0);
         launches++;
@@ -591,7 +601,7 @@ public:
         int nt = 256;
         for (;;) {
             smem = sizeof(cplx<R>) * ((size_t)T * E + (size_t)(nt / T) * xrow_stride<T, E>() + (size_t)np_slots * E * nt) +
-                   (np_slots ? sizeof(R) * (size_t)E * nt : 0);
+                   (np_slots ? 2 * sizeof(R) * (size_t)E * nt : 0);
             if (smem <= 110 * 1024 || nt <= T) break;
             nt /= 2;
         }
@@ -613,6 +623,29 @@ public:
         return cb() * g.nkxc * (double)g.ny * g.nz * (nin + nout) + sizeof(R) * (double)ncell * nreal;
     }
 
+    // persistent TMA-fed x pass: rows per batch, ring geometry, grid
+    template <int T, int E, class K>
+    bool tma_config(K k, int stages, int nslots, bool scal, int &rb, RingGeom &rg, size_t &sm, int &grid)
+    {
+        rb = 128 / T;
+        rg.kp = ring_kp(g.nkxc, T);
+        rg.seg = (unsigned)(sizeof(cplx<R>) * ((g.nkxc + 1) / 2 * 2));
+        rg.stages = stages;
+        for (;;) {
+            sm = tma_smem<R, T, E>(rb, rg, nslots, scal);
+            if (sm <= (size_t)smem_optin || rb * T <= 32) break;
+            rb /= 2;
+        }
+        if (sm > (size_t)smem_optin) return false;
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, rb * T, sm);
+        if (per_sm < 1) return false;
+        const int nbatch = (g.ny * g.nz + rb - 1) / rb;
+        grid = std::min(nbatch, per_sm * num_sms);
+        return true;
+    }
+
     // fast phase-A x pass (3-D); uonly: u only (relaxation finish)
     void xa_launch(int nin, int nout, const PWA<R> &pw, bool grad, bool uonly, const char *name, int nreal)
     {
@@ -627,9 +660,28 @@ public:
                 const int rb = nt / T;
                 launch(name, xbytes(nin, nout, nreal), [&] { k<<<(nrows + rb - 1) / rb, nt, sm, st>>>(g, a, twx, pw); });
             };
-            if (uonly) go(xa_fast<R, T, E, 3, false, true>, 2);
-            else if (grad) go(xa_fast<R, T, E, 3, true, false>, 4);
-            else go(xa_fast<R, T, E, 3, false, false>, 2);
+            auto go_tma = [&](auto k, int np) -> bool {
+                int rb, grid;
+                RingGeom rg;
+                size_t sm;
+                if (!tma_config<T, E>(k, np + 1, np, true, rb, rg, sm, grid)) return false;
+                PairList pl;
+                pl.n = np;
+                for (int p = 0; p < np; ++p) {
+                    pl.fa[p] = (signed char)(2 * p);
+                    pl.fb[p] = (signed char)(2 * p + 1 < nin ? 2 * p + 1 : -1);
+                }
+                launch(name, xbytes(nin, nout, nreal),
+                       [&] { k<<<grid, rb * T, sm, st>>>(g, a, twx, pw, rb, rg, pl); });
+                return true;
+            };
+            if (uonly) {
+                if (!(tma_x && go_tma(xa_tma<R, T, E, false, true>, 2))) go(xa_fast<R, T, E, 3, false, true>, 2);
+            } else if (grad) {
+                if (!(tma_x && go_tma(xa_tma<R, T, E, true, false>, 4))) go(xa_fast<R, T, E, 3, true, false>, 4);
+            } else {
+                if (!(tma_x && go_tma(xa_tma<R, T, E, false, false>, 2))) go(xa_fast<R, T, E, 3, false, false>, 2);
+            }
         });
     }
 
@@ -646,8 +698,34 @@ public:
                 const int rb = nt / T;
                 launch("xpass_b", xbytes(nin, nout, nreal), [&] { k<<<(nrows + rb - 1) / rb, nt, sm, st>>>(g, a, twx, pw); });
             };
-            if (ph.evolve) go(xb_fast<R, T, E, 3, true>);
-            else go(xb_fast<R, T, E, 3, false>);
+            auto go_tma = [&](auto k) -> bool {
+                int rb, grid;
+                RingGeom rg;
+                size_t sm;
+                if (!tma_config<T, E>(k, 4, 0, false, rb, rg, sm, grid)) return false;
+                PairList pl;
+                int np = 0;
+                for (int i = 0; i < nm; i += 2) {
+                    pl.fa[np] = (signed char)i;
+                    pl.fb[np] = (signed char)(i + 1 < nm ? i + 1 : -1);
+                    ++np;
+                }
+                if (ph.evolve)
+                    for (int q = 0; q < 3 * nm; ++q) {
+                        pl.fa[np] = (signed char)(nm + 2 * q);
+                        pl.fb[np] = (signed char)(nm + 2 * q + 1);
+                        ++np;
+                    }
+                pl.n = np;
+                launch("xpass_b", xbytes(nin, nout, nreal),
+                       [&] { k<<<grid, rb * T, sm, st>>>(g, a, twx, pw, rb, rg, pl); });
+                return true;
+            };
+            if (ph.evolve) {
+                if (!(tma_x && go_tma(xb_tma<R, T, E, true>))) go(xb_fast<R, T, E, 3, true>);
+            } else {
+                if (!(tma_x && go_tma(xb_tma<R, T, E, false>))) go(xb_fast<R, T, E, 3, false>);
+            }
         });
     }
 
@@ -751,6 +829,7 @@ public:
         pw.ex = ex; pw.ey = ey; pw.ez = ez;
         pw.ctrl = ctrl;
         pw.stage = stage;
+        pw.status = &ctrl->status;
         const int nout = nm + (ph.evolve ? 6 : 0);
         if (fast_x) xb_launch(nf, nout, pw, ph.evolve ? 1 + nm : 1);
         else xpass(nf, nout, pw, xrb_b, "xpass_b", ph.evolve ? 1 + nm : 1);

@@ -16,7 +16,7 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "lib", "libhydft_gpu.so")
+LIB_PATH = os.environ.get("HYDFT_LIB") or os.path.join(_HERE, "lib", "libhydft_gpu.so")
 
 _D, _I, _P = C.c_double, C.c_int, C.c_void_p
 
