@@ -417,6 +417,18 @@ int hydft_gpu_hnc_solve(const char *potential, double gamma, double kappa, doubl
     return HYDFT_OK;
 }
 
+int hydft_gpu_fourier_bessel(const double *f_in, double *f_out, int n, double rmax, int direction, int device)
+{
+    if (!f_in || !f_out || n < 1 || !(rmax > 0.0) || (direction != 0 && direction != 1)) {
+        g_create_err = "fourier_bessel: bad arguments";
+        return HYDFT_ERR_BAD_ARG;
+    }
+    std::string err;
+    int rc = gpu_fourier_bessel(device, f_in, f_out, n, rmax, direction, err);
+    if (rc) g_create_err = err;
+    return rc;
+}
+
 int hydft_gpu_fd_table(int device, double *out, int *ntab)
 {
     std::vector<double> t;

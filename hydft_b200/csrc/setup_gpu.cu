@@ -383,6 +383,51 @@ static void dst(HncDev &d, const double *x, const double *pre, const double *pos
     dst_kernel<<<(n + 127) / 128, 128, sm>>>(x, pre, post, y, n, d.sintab);
 }
 
+// Fourier-Bessel transform pair of fourier_bessel_t (oz_hnc.f90:79-96) on
+// host arrays: direction 0 is r2k, f(k) = 2 pi dr DST(r f)/k; direction 1
+// is k2r, f(r) = dk DST(k f)/(4 pi^2 r); r_j = j dr, k_m = m dk,
+// dr = rmax/(n+1), dk = pi/((n+1) dr).
+int gpu_fourier_bessel(int device, const double *fin, double *fout, int n, double rmax, int direction,
+                       std::string &err)
+{
+    CKS(cudaSetDevice(device));
+    if (n < 1) { err = "fourier_bessel: n must be >= 1"; return 1; }
+    const size_t smd = sizeof(double) * (2 * ((size_t)n + 1) + n);
+    if (smd > 227 * 1024) { err = "fourier_bessel: n too large for the on-chip sine table (n <= 9600)"; return 8; }
+    const double dr = rmax / (n + 1), dk = PI / ((n + 1) * dr);
+    std::vector<double> pre(n), post(n), sn(2 * (size_t)(n + 1));
+    for (int j = 0; j < n; ++j) {
+        const double r = (j + 1) * dr, k = (j + 1) * dk;
+        pre[j] = direction == 0 ? r : k;
+        post[j] = direction == 0 ? 2.0 * PI * dr / k : dk / (4.0 * PI * PI * r);
+    }
+    for (size_t m = 0; m < sn.size(); ++m) sn[m] = std::sin(PI * (double)m / (double)(n + 1));
+    double *dx = nullptr, *dpre = nullptr, *dpost = nullptr, *dout = nullptr, *dsn = nullptr;
+    int rc = 0;
+    do {
+        if (cudaMalloc(&dx, sizeof(double) * n) != cudaSuccess || cudaMalloc(&dpre, sizeof(double) * n) != cudaSuccess ||
+            cudaMalloc(&dpost, sizeof(double) * n) != cudaSuccess || cudaMalloc(&dout, sizeof(double) * n) != cudaSuccess ||
+            cudaMalloc(&dsn, sizeof(double) * sn.size()) != cudaSuccess) {
+            err = "fourier_bessel: device allocation failed";
+            rc = 2;
+            break;
+        }
+        cudaMemcpy(dx, fin, sizeof(double) * n, cudaMemcpyHostToDevice);
+        cudaMemcpy(dpre, pre.data(), sizeof(double) * n, cudaMemcpyHostToDevice);
+        cudaMemcpy(dpost, post.data(), sizeof(double) * n, cudaMemcpyHostToDevice);
+        cudaMemcpy(dsn, sn.data(), sizeof(double) * sn.size(), cudaMemcpyHostToDevice);
+        cudaFuncSetAttribute(dst_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smd, 48 * 1024));
+        dst_kernel<<<(n + 127) / 128, 128, smd>>>(dx, dpre, dpost, dout, n, dsn);
+        cudaError_t e = cudaMemcpy(fout, dout, sizeof(double) * n, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) {
+            err = std::string("fourier_bessel: ") + cudaGetErrorString(e);
+            rc = 7;
+        }
+    } while (0);
+    cudaFree(dx); cudaFree(dpre); cudaFree(dpost); cudaFree(dout); cudaFree(dsn);
+    return rc;
+}
+
 static int run_direct(HncDev &d, const Potential &pot, double n0, double rmax, double tol, double mix,
                       int maxiter, const double *gamma_s_init, HncOut &res, bool &unstable_out,
                       std::string &err)

@@ -26,6 +26,8 @@ void gauss_legendre(int n, double *x, double *w);
 int gpu_fd_table(int device, std::vector<double> &out, std::string &err);
 int gpu_fd_alpha(int device, const std::vector<double> &tab, const double *y, double *alpha, int n,
                  std::string &err);
+int gpu_fourier_bessel(int device, const double *fin, double *fout, int n, double rmax, int direction,
+                       std::string &err);
 int gpu_hnc_solve(int device, const Potential &pot, double n0, int nr, double rmax, double tol, double mix,
                   int maxiter, HncOut &res, std::string &err);
 

@@ -113,6 +113,7 @@ def lib():
         L.hydft_gpu_hnc_solve.argtypes = [C.c_char_p, _D, _D, _D, _D, _I, _D, _D, _D, _I, _I,
                                           _P, _P, _P, _P, _P, C.POINTER(_D), C.POINTER(_I),
                                           C.POINTER(_I), C.POINTER(_D)]
+        L.hydft_gpu_fourier_bessel.argtypes = [_P, _P, _I, _D, _I, _I]
         L.hydft_gpu_fd_table.argtypes = [_I, _P, C.POINTER(_I)]
         L.hydft_gpu_fd_alpha.argtypes = [_I, _P, _P, _I]
         _lib = L
@@ -334,6 +335,16 @@ def hnc_solve(potential, gamma, kappa, lam, n0, nr, rmax, tol, mix, maxiter, dev
     if rc:
         raise HydftError(rc, lib().hydft_gpu_create_error().decode())
     out.update(u_ex=u.value, converged=bool(conv.value), niter=nit.value, residual=res.value)
+    return out
+
+
+def fourier_bessel(f, rmax, direction, device=0):
+    """fourier_bessel_t%r2k (direction 0) / %k2r (1) of a length-n array."""
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    out = np.zeros_like(f)
+    rc = lib().hydft_gpu_fourier_bessel(_ptr(f), _ptr(out), f.size, float(rmax), int(direction), device)
+    if rc:
+        raise HydftError(rc, lib().hydft_gpu_create_error().decode())
     return out
 
 

@@ -211,6 +211,15 @@ int hydft_gpu_hnc_solve(const char *potential, double gamma, double kappa, doubl
                         int device, double *r, double *k, double *g, double *ck, double *sk,
                         double *u_ex, int *converged, int *niter, double *residual);
 
+/* Fourier-Bessel transform pair of the HNC solver (fourier_bessel_t%r2k /
+ * %k2r, src/structure/oz_hnc.f90:79-96) on the GPU in FP64, host arrays of
+ * length n: direction 0 is r2k, f(k) = (4 pi/k) int r f(r) sin(kr) dr;
+ * direction 1 is k2r, f(r) = (1/(2 pi^2 r)) int k f(k) sin(kr) dk; on the
+ * grids r_j = j dr, k_m = m dk, dr = rmax/(n+1), dk = pi/((n+1) dr).
+ * n <= 9600. */
+int hydft_gpu_fourier_bessel(const double *f_in, double *f_out, int n, double rmax, int direction,
+                             int device);
+
 /* Fermi-Dirac table tab(6, 6601) (fermi_dirac.f90:30-74) built on the GPU;
  * out has 6*6601 doubles, column index fastest. */
 int hydft_gpu_fd_table(int device, double *out, int *ntab);

@@ -74,6 +74,23 @@ def test_fd_table_and_inverse(hg, orc):
     assert np.abs(al - ao).max() < 1e-9 * max(1.0, np.abs(ao).max())
 
 
+def test_fourier_bessel_matches_oracle(hg, orc):
+    from hydft_b200 import model
+    nr, rmax = 4096, 60.0
+    dr = rmax / (nr + 1)
+    r = dr * np.arange(1, nr + 1)
+    k = np.pi / ((nr + 1) * dr) * np.arange(1, nr + 1)
+    fr = np.exp(-r)
+    fk = model.fourier_bessel(fr, rmax, 0)
+    assert np.abs(fk - orc.fb_r2k(fr, rmax)).max() < 1e-12 * np.abs(fk).max()
+    # test_hnc.f90:25-35: transform of exp(-r) and the round trip
+    sel = k < 20.0
+    assert np.abs(fk[sel] * (k[sel] ** 2 + 1) ** 2 / (8 * np.pi) - 1).max() < 1e-4
+    back = model.fourier_bessel(fk, rmax, 1)
+    assert np.abs(back - orc.fb_k2r(fk, rmax)).max() < 1e-12 * np.abs(back).max()
+    assert np.abs(back - fr).max() < 1e-12
+
+
 @pytest.mark.parametrize("pot,gam,kap,lam", [("yukawa", 10.0, 1.0, 1.0), ("coulomb", 10.0, 0.0, 1.0),
                                              ("hansen_mcdonald", 0.5, 0.0, 2 * np.sqrt(np.pi * 0.5))])
 def test_hnc_matches_oracle(hg, orc, pot, gam, kap, lam):
