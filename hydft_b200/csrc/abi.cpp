@@ -25,6 +25,11 @@ struct hydft_gpu {
 
 static thread_local std::string g_create_err;
 
+namespace hydft {
+// message of a failed handle-less call, returned by hydft_gpu_create_error()
+void set_thread_error(const std::string &msg) { g_create_err = msg; }
+}  // namespace hydft
+
 static int fail(hydft_gpu *h, int rc, const std::string &msg)
 {
     if (h) h->err = msg;

@@ -220,6 +220,27 @@ int hydft_gpu_hnc_solve(const char *potential, double gamma, double kappa, doubl
 int hydft_gpu_fourier_bessel(const double *f_in, double *f_out, int n, double rmax, int direction,
                              int device);
 
+/*
+ * hydft_gpu_fourier_bessel without device allocation.  No counterpart in
+ * the reference: it exists for callers that cannot allocate device memory
+ * where they need the transform (inside a loop that must not synchronise
+ * the device, or under a host framework that owns all device allocations).
+ * d_in and d_out are device arrays of n doubles provided by the caller; the
+ * sine table and weights live in a fixed scratch array inside the library
+ * (2(n+1) + 2n doubles for n <= HYDFT_FB_NOALLOC_MAX_N, 262 160 bytes,
+ * resident on every GPU that loads the library until the process exits).
+ * n above the maximum is rejected with HYDFT_ERR_BAD_ARG.  The kernels run
+ * on `stream` (a cudaStream_t; NULL for the default stream) and the call
+ * returns without waiting for them.  Every call rebuilds the tables for its
+ * own n and rmax; calls whose work overlaps on the GPU share the scratch
+ * array and race.  The first call on a device looks up the scratch array's
+ * address and configures the kernel; make it before any stream capture.
+ * Errors: hydft_gpu_create_error().
+ */
+#define HYDFT_FB_NOALLOC_MAX_N 8192
+int hydft_gpu_fourier_bessel_noalloc(const double *d_in, double *d_out, int n, double rmax,
+                                     int direction, void *stream);
+
 /* Fermi-Dirac table tab(6, 6601) (fermi_dirac.f90:30-74) built on the GPU;
  * out has 6*6601 doubles, column index fastest. */
 int hydft_gpu_fd_table(int device, double *out, int *ntab);
