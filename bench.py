@@ -53,7 +53,7 @@ def initial_density(n, L, n0, seed=2024):
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -61,12 +61,17 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.lines = []
+        self.window = None
+
+    def mark(self, t0, t1):
+        """Keep only the samples taken between wall-clock times t0 and t1."""
+        self.window = (t0, t1)
 
     def start(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except OSError:
@@ -84,18 +89,34 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
+        out = self._summary(self.window)
+        if out is None and self.window is not None:
+            out = self._summary(None)
+            if out is not None:
+                out["window"] = "no sample inside the timed region; all samples"
+        return out
+
+    def _summary(self, window):
+        import datetime
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
             parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
+            if window is not None:
+                try:
+                    ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                except ValueError:
+                    continue
+                if not (window[0] - 0.05 <= ts <= window[1] + 0.05):
+                    continue
             try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
+                sm.append(float(parts[2]))
+                smax.append(float(parts[3]))
             except ValueError:
                 continue
-            for nm, v in zip(names, parts[5:9]):
+            for nm, v in zip(names, parts[6:10]):
                 if v.lower() == "active":
                     reasons.add(nm)
         if not sm:
@@ -191,7 +212,7 @@ def structure_for_workload(hg, device):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256)
@@ -248,11 +269,14 @@ def main():
     e1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize(dev)
     barrier()
+    w0 = time.time()
     e0.record(stream)
     m32.advance(args.steps)
     e1.record(stream)
     torch.cuda.synchronize(dev)
+    w1 = time.time()
     barrier()
+    clocks.mark(w0, w1)
     ck = clocks.stop()
     ms = e0.elapsed_time(e1)
     gpu_launches = m32.launch_count() - launches0

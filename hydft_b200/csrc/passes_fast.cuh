@@ -24,14 +24,14 @@ __global__ void __launch_bounds__(TX * T * G) zinv_fast(Grid g, PassArgs<R> a, c
     constexpr int L = T * E;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
-    cplx<R> *xb = tw + L;
+    cplx<R> *xb = tw + 2 * L;
     const int tid = threadIdx.x, c = tid % TX, t = (tid / TX) % T, gi = tid / (TX * T);
     const int x = blockIdx.x * TX + c, kyc = blockIdx.y * G + gi, f = blockIdx.z;
     const bool valid = x < g.nkxc && kyc < g.nkyc;
     const cplx<R> *__restrict__ in = a.in[f];
     cplx<R> *__restrict__ out = a.out[f];
     const int op = a.op[f];
-    for (int i = tid; i < L; i += blockDim.x) tw[i] = twz[i];
+    for (int i = tid; i < 2 * L; i += blockDim.x) tw[i] = twz[i];
     const int my = valid ? signed_idx(kyc, g.My) : 0;
     const R kx = R(x * g.kx0), ky = R(my * g.ky0);
     cplx<R> v[E];
@@ -85,13 +85,13 @@ __global__ void __launch_bounds__(TX * T * G) yinv_fast(Grid g, PassArgs<R> a, c
     constexpr int L = T * E;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
-    cplx<R> *xb = tw + L;
+    cplx<R> *xb = tw + 2 * L;
     const int tid = threadIdx.x, c = tid % TX, t = (tid / TX) % T, gi = tid / (TX * T);
     const int x = blockIdx.x * TX + c, z = blockIdx.y * G + gi, f = blockIdx.z;
     const bool valid = x < g.nkxc && z < g.nz;
     const cplx<R> *__restrict__ in = a.in[f];
     cplx<R> *__restrict__ out = a.out[f];
-    for (int i = tid; i < L; i += blockDim.x) tw[i] = twy[i];
+    for (int i = tid; i < 2 * L; i += blockDim.x) tw[i] = twy[i];
     cplx<R> v[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) {
@@ -120,13 +120,13 @@ __global__ void __launch_bounds__(TX * T * G) yfwd_fast(Grid g, PassArgs<R> a, c
     constexpr int L = T * E;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
-    cplx<R> *xb = tw + L;
+    cplx<R> *xb = tw + 2 * L;
     const int tid = threadIdx.x, c = tid % TX, t = (tid / TX) % T, gi = tid / (TX * T);
     const int x = blockIdx.x * TX + c, z = blockIdx.y * G + gi, f = blockIdx.z;
     const bool valid = x < g.nkxc && z < g.nz;
     const cplx<R> *__restrict__ in = a.in[f];
     cplx<R> *__restrict__ out = a.out[f];
-    for (int i = tid; i < L; i += blockDim.x) tw[i] = twy[i];
+    for (int i = tid; i < 2 * L; i += blockDim.x) tw[i] = twy[i];
     cplx<R> v[E];
 #pragma unroll
     for (int r = 0; r < E; ++r) {
@@ -153,13 +153,13 @@ __global__ void __launch_bounds__(TX * T * G) zfwd_fast(Grid g, PassArgs<R> a, c
     constexpr int L = T * E;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
-    cplx<R> *xb = tw + L;
+    cplx<R> *xb = tw + 2 * L;
     const int tid = threadIdx.x, c = tid % TX, t = (tid / TX) % T, gi = tid / (TX * T);
     const int x = blockIdx.x * TX + c, kyc = blockIdx.y * G + gi, f = blockIdx.z;
     const bool valid = x < g.nkxc && kyc < g.nkyc;
     const cplx<R> *__restrict__ in = a.in[f];
     cplx<R> *__restrict__ out = a.out[f];
-    for (int i = tid; i < L; i += blockDim.x) tw[i] = twz[i];
+    for (int i = tid; i < 2 * L; i += blockDim.x) tw[i] = twz[i];
     cplx<R> v[E];
 #pragma unroll
     for (int r = 0; r < E; ++r) {
@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(TX * T * G) zfwd_fast(Grid g, PassArgs<R> a, c
 template <typename R>
 inline size_t yz_fast_smem(int L, int T, int TX, int G)
 {
-    return sizeof(cplx<R>) * ((size_t)L + (size_t)G * (L + L / T) * TX);
+    return sizeof(cplx<R>) * (2 * (size_t)L + (size_t)G * (L + L / T) * TX);
 }
 
 // --------------------------------------------------------------- x passes
@@ -281,7 +281,7 @@ __global__ void __launch_bounds__(256, HYDFT_XMINB) xa_fast(Grid g, XFastArgs<R>
     constexpr int NOUT = UONLY ? NM : NM + NF + 1;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
-    cplx<R> *xbuf = tw + L;
+    cplx<R> *xbuf = tw + 2 * L;
     const int nt = blockDim.x, rb = nt / T;
     cplx<R> *slots = xbuf + rb * xrow_stride<T, E>();
     R *muslot = reinterpret_cast<R *>(slots + NP * E * nt);
@@ -290,7 +290,7 @@ __global__ void __launch_bounds__(256, HYDFT_XMINB) xa_fast(Grid g, XFastArgs<R>
     const int row = blockIdx.x * rb + rr;
     const bool rowok = row < g.ny * g.nz;
     cplx<R> *xrow = xbuf + rr * xrow_stride<T, E>();
-    for (int i = tid; i < L; i += nt) tw[i] = twx[i];
+    for (int i = tid; i < 2 * L; i += nt) tw[i] = twx[i];
     __syncthreads();
 #pragma unroll 1
     for (int p = 0; p < NP; ++p) {
@@ -390,13 +390,13 @@ __global__ void __launch_bounds__(256, HYDFT_XMINB) xb_fast(Grid g, XFastArgs<R>
     constexpr int L = T * E;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
-    cplx<R> *xbuf = tw + L;
+    cplx<R> *xbuf = tw + 2 * L;
     const int nt = blockDim.x, rb = nt / T;
     const int tid = threadIdx.x, t = tid % T, rr = tid / T;
     const int row = blockIdx.x * rb + rr;
     const bool rowok = row < g.ny * g.nz;
     cplx<R> *xrow = xbuf + rr * xrow_stride<T, E>();
-    for (int i = tid; i < L; i += nt) tw[i] = twx[i];
+    for (int i = tid; i < 2 * L; i += nt) tw[i] = twx[i];
     __syncthreads();
     const R nref = pw.nhat[0].x;
     const size_t rowbase = (size_t)row * g.nx;
@@ -449,6 +449,245 @@ __global__ void __launch_bounds__(256, HYDFT_XMINB) xb_fast(Grid g, XFastArgs<R>
     }
 }
 
+// 16-byte asynchronous global -> shared copies (cp.async, sm_80 and later);
+// the wait only covers this thread's own committed copies, so it ends.
+__device__ __forceinline__ void cp_async16(void *dst_smem, const void *src_gmem)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src_gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// bulk prefetch of a 16-byte aligned global range (a multiple of 16 bytes)
+// into L2; no completion to wait for
+__device__ __forceinline__ void prefetch_l2(const void *p, unsigned bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// The spectral input rows of one block of x rows are contiguous in every
+// field (row stride pkx).  XPrefetch keeps the rows of the next fields in
+// flight to L2 (thread 0 of the block issues one bulk prefetch per field)
+// while the current field pair is transformed.
+template <typename R>
+struct XPrefetch {
+    const XFastArgs<R> &a;
+    size_t off;
+    unsigned bytes;
+    int next = 0;
+    bool issuer;
+    __device__ XPrefetch(const XFastArgs<R> &a_, const Grid &g, int row0, int rows, bool is0)
+        : a(a_), off((size_t)row0 * g.pkx), bytes((unsigned)((size_t)rows * g.pkx * sizeof(cplx<R>))), issuer(is0) {}
+    // prefetch every field up to index f (inclusive)
+    __device__ __forceinline__ void upto(int f)
+    {
+        for (; next <= f && next < a.nin; ++next)
+            if (issuer && bytes) prefetch_l2(a.in[next] + off, bytes);
+    }
+};
+
+// blocks per SM the staged x passes are compiled for: two 256-thread blocks
+// in single precision with up to 16 values per thread, else one
+template <typename R, int E>
+__host__ __device__ constexpr int xstaged_minb() { return sizeof(R) == 4 && E <= 16 ? 2 : 1; }
+
+// Phase A without Fermi-Dirac terms (ideal / Hartree / RY ions and the u-only
+// relaxation finish): the four inputs dn, m_0..m_2 stay in registers as two
+// pairs, so no per-thread shared-memory slots are needed and two 256-thread
+// blocks fit on an SM.  The output pairs are ordered so that dn is consumed
+// first: (mu_local, u_0), (u_1, u_2), (m0u0, m0u1), (m0u2, m1u1), (m1u2, m2u2);
+// UONLY: (u_0, u_1), (u_2, -).  Outputs go to the same fields as xa_fast's.
+template <typename R, int T, int E, bool UONLY>
+__global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xa_regs(Grid g, XFastArgs<R> a, const cplx<R> *twx, PWA<R> pw)
+{
+    constexpr int L = T * E;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
+    cplx<R> *xbuf = tw + 2 * L;
+    const int nt = blockDim.x, rb = nt / T;
+    const int tid = threadIdx.x, t = tid % T, rr = tid / T;
+    const int row = blockIdx.x * rb + rr;
+    const bool rowok = row < g.ny * g.nz;
+    cplx<R> *xrow = xbuf + rr * xrow_stride<T, E>();
+    {
+        const int row0 = blockIdx.x * rb;
+        XPrefetch<R> pf(a, g, row0, max(0, min(rb, g.ny * g.nz - row0)), tid == 0);
+        pf.upto(3);
+    }
+    for (int i = tid; i < 2 * L; i += nt) tw[i] = twx[i];
+    __syncthreads();
+    cplx<R> p0[E], p1[E];   // (dn, m_0), (m_1, m_2)
+    x_c2r_pair<R, T, E>(p0, a.in[0], a.in[1], row, rowok, t, g, xrow, tw);
+    x_c2r_pair<R, T, E>(p1, a.in[2], a.in[3], row, rowok, t, g, xrow, tw);
+    const R nref = pw.nhat[0].x;
+    const R inv_nref = R(1) / nref, inv_beta = R(pw.ph.inv_beta), mass = R(pw.ph.mass);
+    const size_t rowbase = (size_t)row * g.nx;
+    // mu_local (ideal terms in the given order) and 1/(m n); p0[r].x becomes 1/(m n)
+    cplx<R> v[E];
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+        const int xx = block_pos<T, E>(t, r);
+        const R dn = p0[r].x;
+        const R n = nref + dn;
+        const R inv_mn = R(1) / (mass * n);
+        if (rowok) {
+            if (!(n > R(0))) atomicOr(pw.status, isfinite(n) ? ST_NONPOS : ST_NONFINITE);
+            if (pw.dn_real) pw.dn_real[rowbase + xx] = dn;
+            if (pw.u_real) {
+                pw.u_real[rowbase + xx] = p0[r].y * inv_mn;
+                pw.u_real[pw.ncell + rowbase + xx] = p1[r].x * inv_mn;
+                pw.u_real[2 * pw.ncell + rowbase + xx] = p1[r].y * inv_mn;
+            }
+        }
+        if (!UONLY) {
+            R mu = R(0);
+            for (int tt = 0; tt < pw.ph.nterms_local; ++tt)
+                if (pw.ph.term_order[tt] == 1) mu += log1p(dn * inv_nref) * inv_beta;
+            v[r] = cplx<R>{mu, p0[r].y * inv_mn};
+        } else {
+            v[r] = cplx<R>{p0[r].y * inv_mn, p1[r].x * inv_mn};
+        }
+        p0[r].x = inv_mn;
+    }
+    if (!UONLY) {
+        // outputs: 0..2 u_d, 3..8 fluxes (00, 01, 02, 11, 12, 22), 9 mu
+        x_r2c_pair<R, T, E>(v, a.out[9], a.out[0], row, rowok, t, g, xrow, tw);
+#pragma unroll
+        for (int r = 0; r < E; ++r) v[r] = cplx<R>{p1[r].x * p0[r].x, p1[r].y * p0[r].x};
+        x_r2c_pair<R, T, E>(v, a.out[1], a.out[2], row, rowok, t, g, xrow, tw);
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+            const R u0 = p0[r].y * p0[r].x;
+            v[r] = cplx<R>{p0[r].y * u0, p0[r].y * (p1[r].x * p0[r].x)};
+        }
+        x_r2c_pair<R, T, E>(v, a.out[3], a.out[4], row, rowok, t, g, xrow, tw);
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+            const R u1 = p1[r].x * p0[r].x, u2 = p1[r].y * p0[r].x;
+            v[r] = cplx<R>{p0[r].y * u2, p1[r].x * u1};
+        }
+        x_r2c_pair<R, T, E>(v, a.out[5], a.out[6], row, rowok, t, g, xrow, tw);
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+            const R u2 = p1[r].y * p0[r].x;
+            v[r] = cplx<R>{p1[r].x * u2, p1[r].y * u2};
+        }
+        x_r2c_pair<R, T, E>(v, a.out[7], a.out[8], row, rowok, t, g, xrow, tw);
+    } else {
+        x_r2c_pair<R, T, E>(v, a.out[0], a.out[1], row, rowok, t, g, xrow, tw);
+#pragma unroll
+        for (int r = 0; r < E; ++r) v[r] = cplx<R>{p1[r].y * p0[r].x, R(0)};
+        x_r2c_pair<R, T, E>(v, a.out[2], nullptr, row, rowok, t, g, xrow, tw);
+    }
+}
+
+// row stride (elements) of the staged real rows: one row of x plus T, so
+// that the rows read by one warp start in different bank groups
+template <int T, int E>
+__host__ __device__ constexpr int xreal_stride() { return T * E + T; }
+
+// Phase B with this block's real-space rows (dn and, when Pi evolves, u_d)
+// copied into shared memory by cp.async at the start; the copies overlap the
+// first inverse transform, and the spectral inputs are prefetched to L2 a few
+// fields ahead.  Same inputs, outputs and arithmetic as xb_fast.
+template <typename R, int T, int E, bool EVOLVE, bool EXT>
+__global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xb_rows(Grid g, XFastArgs<R> a, const cplx<R> *twx, PWB<R> pw)
+{
+    constexpr int L = T * E, NM = 3;
+    constexpr int RS = xreal_stride<T, E>();
+    constexpr int CPR = L * (int)sizeof(R) / 16;   // 16-byte chunks per row
+    constexpr int EPC = 16 / (int)sizeof(R);        // elements per chunk
+    constexpr int AHEAD = 6;                        // fields prefetched ahead
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
+    cplx<R> *xbuf = tw + 2 * L;
+    const int nt = blockDim.x, rb = nt / T;
+    R *rs = reinterpret_cast<R *>(xbuf + rb * xrow_stride<T, E>());   // [field][rb][RS]
+    const int tid = threadIdx.x, t = tid % T, rr = tid / T;
+    const int nrows = g.ny * g.nz;
+    const int row0 = blockIdx.x * rb;
+    const int row = row0 + rr;
+    const bool rowok = row < nrows;
+    cplx<R> *xrow = xbuf + rr * xrow_stride<T, E>();
+    const int vrows = max(0, min(rb, nrows - row0));
+    {
+        const int nf = EVOLVE ? 1 + NM : 1;
+        const int total = nf * vrows * CPR;
+        for (int i = tid; i < total; i += nt) {
+            const int c = i % CPR, j = (i / CPR) % vrows, f = i / (CPR * vrows);
+            const R *src = (f == 0 ? pw.dn_real : pw.u_real + (size_t)(f - 1) * pw.ncell) + (size_t)(row0 + j) * L + c * EPC;
+            cp_async16(rs + ((size_t)f * rb + j) * RS + c * EPC, src);
+        }
+        cp_async_commit();
+    }
+    XPrefetch<R> pf(a, g, row0, vrows, tid == 0);
+    pf.upto(AHEAD);
+    for (int i = tid; i < 2 * L; i += nt) tw[i] = twx[i];
+    __syncthreads();
+    const R nref = pw.nhat[0].x;
+    const int y = rowok ? row % g.ny : 0, z = rowok ? row / g.ny : 0;
+    const R *nrow = rs + rr * RS;
+    // n (dmu - F): pairs of components
+#pragma unroll
+    for (int q = 0; 2 * q < NM; ++q) {
+        const int i0 = 2 * q, i1 = 2 * q + 1;
+        cplx<R> v[E];
+        pf.upto(i1 + AHEAD);
+        x_c2r_pair<R, T, E>(v, a.in[i0], i1 < NM ? a.in[i1] : nullptr, row, rowok, t, g, xrow, tw);
+        if (q == 0) {
+            cp_async_wait_all();
+            __syncthreads();
+        }
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+            const int xx = block_pos<T, E>(t, r);
+            const R n = nref + nrow[xx];
+            R f0 = R(0), f1 = R(0);
+            if (EXT) {
+                const StageScal &s = pw.ctrl->st[pw.stage];
+                cplx<double> e = pw.ex[xx] * pw.ey[y];
+                e = e * pw.ez[z];
+                e = e * cplx<double>{s.ewr, s.ewi};
+                const double sf = s.amp * e.y;
+                f0 = R(sf * pw.ph.ext_k[i0]);
+                if (i1 < NM) f1 = R(sf * pw.ph.ext_k[i1]);
+            }
+            v[r] = cplx<R>{n * (v[r].x - f0), n * (v[r].y - f1)};
+        }
+        x_r2c_pair<R, T, E>(v, a.out[i0], i1 < NM ? a.out[i1] : nullptr, row, rowok, t, g, xrow, tw);
+    }
+    if (EVOLVE) {
+        // -u.grad Pi for component pairs (0,1), (2,3), (4,5)
+#pragma unroll 1
+        for (int cp = 0; cp < 3; ++cp) {
+            cplx<R> acc[E];
+#pragma unroll
+            for (int r = 0; r < E; ++r) acc[r] = cplx<R>{R(0), R(0)};
+#pragma unroll
+            for (int d = 0; d < NM; ++d) {
+                const int f = NM + 2 * (cp * NM + d);
+                cplx<R> v[E];
+                pf.upto(f + 1 + AHEAD);
+                x_c2r_pair<R, T, E>(v, a.in[f], a.in[f + 1], row, rowok, t, g, xrow, tw);
+                const R *urow = rs + ((1 + d) * rb + rr) * RS;
+#pragma unroll
+                for (int r = 0; r < E; ++r) acc[r] = acc[r] - urow[block_pos<T, E>(t, r)] * v[r];
+            }
+            x_r2c_pair<R, T, E>(acc, a.out[NM + 2 * cp], a.out[NM + 2 * cp + 1], row, rowok, t, g, xrow, tw);
+        }
+    }
+}
+
+// shared-memory bytes of a staged x pass
+template <typename R, int T, int E>
+inline size_t xstaged_smem(int nt, int nreal)
+{
+    const int rb = nt / T;
+    return sizeof(cplx<R>) * (2 * (size_t)T * E + (size_t)rb * xrow_stride<T, E>()) +
+           sizeof(R) * (size_t)nreal * rb * xreal_stride<T, E>();
+}
+
 // Real-space I/O: half spectra -> real fields (TOREAL) or back.
 template <typename R, int T, int E, bool TOREAL>
 __global__ void __launch_bounds__(256) xio_fast(Grid g, XFastArgs<R> a, const cplx<R> *twx, PWToReal<R> dst,
@@ -457,13 +696,13 @@ __global__ void __launch_bounds__(256) xio_fast(Grid g, XFastArgs<R> a, const cp
     constexpr int L = T * E;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
-    cplx<R> *xbuf = tw + L;
+    cplx<R> *xbuf = tw + 2 * L;
     const int nt = blockDim.x, rb = nt / T;
     const int tid = threadIdx.x, t = tid % T, rr = tid / T;
     const int row = blockIdx.x * rb + rr;
     const bool rowok = row < g.ny * g.nz;
     cplx<R> *xrow = xbuf + rr * xrow_stride<T, E>();
-    for (int i = tid; i < L; i += nt) tw[i] = twx[i];
+    for (int i = tid; i < 2 * L; i += nt) tw[i] = twx[i];
     __syncthreads();
     const size_t rowbase = (size_t)row * g.nx;
     const int nf = TOREAL ? a.nin : a.nout;

@@ -124,7 +124,10 @@ struct BarWarp {
 
 // x in stride layout (v[e] = x[t + T e]) -> X in block layout
 // (v[j*T + k1] = X[(t + T j) + E k1]).  `sm` is this column's exchange
-// buffer (element stride ES), `tw` the W_L table.
+// buffer (element stride ES).  `tw` is the planned twiddle table of 2L
+// entries: W_L^{t k2} at [k2 T + t] (k2 < E, t < T) for this routine, then
+// W_L^{k2 m1} at [L + m1 E + k2] (m1 < T, k2 < E) for block_to_stride, laid
+// out so that the T threads of a column read consecutive entries.
 template <int T, int E, int DIR, typename R, class BAR = BarBlock, int ES = 1>
 __device__ __forceinline__ void stride_to_block(cplx<R> (&v)[E], int t, cplx<R> *sm,
                                                 const cplx<R> *__restrict__ tw)
@@ -132,7 +135,7 @@ __device__ __forceinline__ void stride_to_block(cplx<R> (&v)[E], int t, cplx<R> 
     RegDFT<E, DIR, R>::run(v);
 #pragma unroll
     for (int k2 = 1; k2 < E; ++k2) {
-        cplx<R> w = tw[t * k2];   // t*k2 < T*E = L
+        cplx<R> w = tw[k2 * T + t];   // W_L^{t k2}
         if (DIR > 0) w.y = -w.y;
         v[k2] = v[k2] * w;
     }
@@ -170,7 +173,7 @@ __device__ __forceinline__ void block_to_stride(cplx<R> (&v)[E], int t, cplx<R> 
         cplx<R> *wp = sm + (t + j * (T + 1)) * ES;                   // element m1*E + k2
 #pragma unroll
         for (int m1 = 0; m1 < T; ++m1) {
-            cplx<R> w = tw[k2 * m1];   // k2*m1 < E*T = L
+            cplx<R> w = tw[T * E + m1 * E + k2];   // W_L^{k2 m1}
             if (DIR > 0) w.y = -w.y;
             wp[m1 * EP * ES] = m1 == 0 ? u[0] : u[m1] * w;
         }

@@ -24,7 +24,6 @@
 #include "kernels.cuh"
 #include "passes_fast.cuh"
 #include "solver.hpp"
-#include "xpass_tma.cuh"
 
 #include <type_traits>
 
@@ -221,6 +220,7 @@ public:
     double *fdtab = nullptr;
     cplx<double> *ex, *ey, *ez;
     cplx<R> *twx, *twy, *twz;
+    cplx<R> *tpx = nullptr, *tpy = nullptr, *tpz = nullptr;   // planned tables of the register passes
     Ctrl *ctrl;
     RedPart *rpart, *rout;
     int red_blocks = 0;
@@ -230,7 +230,7 @@ public:
     int smem_optin = 0;
     bool host_pending = false;   // a Maxwell relaxation waits for u of the new state
     bool fast_x = false;         // x passes on the register FFT (3-D grids, planned nx)
-    bool tma_x = false;          // persistent TMA-fed x passes (HYDFT_XPASS=tma); measured slower
+    bool staged_x = true;        // xa_regs / xb_rows (HYDFT_XPASS=v1 selects xa_fast / xb_fast)
     int num_sms = 148;
 
     // per-kernel CUDA-event timing (profile mode, uncaptured steps only)
@@ -411,6 +411,30 @@ public:
         if (int rc = up_tw(twx, g.nx)) return rc;
         if (int rc = up_tw(twy, g.ny)) return rc;
         if (int rc = up_tw(twz, g.nz)) return rc;
+        // register-pass tables: W_L^{t k2} at [k2 T + t], then W_L^{k2 m1} at
+        // [L + m1 E + k2], entries of the W_L table above
+        auto up_tp = [&](cplx<R> *&dst, int L) -> int {
+            int rc = 0;
+            with_plan(L, [&](auto Tc, auto Ec) {
+                constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value;
+                std::vector<cplx<R>> tw, tp(2 * (size_t)L);
+                make_twiddles<R>(L, tw);
+                for (int k2 = 0; k2 < E; ++k2)
+                    for (int t = 0; t < T; ++t) tp[k2 * T + t] = tw[(t * k2) % L];
+                for (int m1 = 0; m1 < T; ++m1)
+                    for (int k2 = 0; k2 < E; ++k2) tp[L + m1 * E + k2] = tw[(k2 * m1) % L];
+                if ((rc = alloc(dst, tp.size()))) return;
+                const cudaError_t e = cudaMemcpy(dst, tp.data(), tp.size() * sizeof(cplx<R>), cudaMemcpyHostToDevice);
+                if (e != cudaSuccess) {
+                    err = std::string("cudaMemcpy (register-pass twiddles): ") + cudaGetErrorString(e);
+                    rc = HYDFT_E_CUDA;
+                }
+            });
+            return rc;
+        };
+        if (int rc = up_tp(tpx, g.nx)) return rc;
+        if (int rc = up_tp(tpy, g.ny)) return rc;
+        if (int rc = up_tp(tpz, g.nz)) return rc;
         if (int rc = alloc(ctrl, 1)) return rc;
         {
             Ctrl c;
@@ -444,7 +468,7 @@ public:
         fast_x = has_plan(g.nx) && nm == 3;
         {
             const char *ev = std::getenv("HYDFT_XPASS");
-            if (ev && std::string(ev) == "tma") tma_x = true;
+            if (ev && std::string(ev) == "v1") staged_x = false;
             CK(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
         }
         // uniform initial state n = n0, mom = 0, Pi = 0 (species.f90:155-169)
@@ -507,7 +531,7 @@ public:
             auto k = zinv_fast<R, T, E, TX, G>;
             set_smem(k, sm);
             const dim3 grid((g.nkxc + TX - 1) / TX, (g.nkyc + G - 1) / G, nf);
-            launch("zinv", zbytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, a, twz); });
+            launch("zinv", zbytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, a, tpz); });
         });
         if (!zf) {
             const int ntx = (g.nkxc + TX - 1) / TX;
@@ -530,7 +554,7 @@ public:
                 auto k = yinv_fast<R, T, E, TX, G>;
                 set_smem(k, sm);
                 const dim3 grid((g.nkxc + TX - 1) / TX, (g.nz + G - 1) / G, nf);
-                launch("yinv", ybytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, b, twy); });
+                launch("yinv", ybytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, b, tpy); });
             });
             if (!yf) {
                 const int ntx = (g.nkxc + TX - 1) / TX;
@@ -561,7 +585,7 @@ public:
                 auto k = yfwd_fast<R, T, E, TX, G>;
                 set_smem(k, sm);
                 const dim3 grid((g.nkxc + TX - 1) / TX, (g.nz + G - 1) / G, nf);
-                launch("yfwd", ybytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, b, twy); });
+                launch("yfwd", ybytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, b, tpy); });
             });
             if (!yf) {
                 const size_t smy = sizeof(cplx<R>) * (2 * (size_t)g.ny * TX + g.ny);
@@ -585,7 +609,7 @@ public:
             auto k = zfwd_fast<R, T, E, TX, G>;
             set_smem(k, sm);
             const dim3 grid((g.nkxc + TX - 1) / TX, (g.nkyc + G - 1) / G, nf);
-            launch("zfwd", zbytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, a, twz, norm); });
+            launch("zfwd", zbytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, a, tpz, norm); });
         });
         if (!zf) {
             const size_t smz = sizeof(cplx<R>) * (2 * (size_t)g.nz * TX + g.nz);
@@ -600,7 +624,7 @@ public:
     {
         int nt = 256;
         for (;;) {
-            smem = sizeof(cplx<R>) * ((size_t)T * E + (size_t)(nt / T) * xrow_stride<T, E>() + (size_t)np_slots * E * nt) +
+            smem = sizeof(cplx<R>) * (2 * (size_t)T * E + (size_t)(nt / T) * xrow_stride<T, E>() + (size_t)np_slots * E * nt) +
                    (np_slots ? 2 * sizeof(R) * (size_t)E * nt : 0);
             if (smem <= 110 * 1024 || nt <= T) break;
             nt /= 2;
@@ -623,29 +647,6 @@ public:
         return cb() * g.nkxc * (double)g.ny * g.nz * (nin + nout) + sizeof(R) * (double)ncell * nreal;
     }
 
-    // persistent TMA-fed x pass: rows per batch, ring geometry, grid
-    template <int T, int E, class K>
-    bool tma_config(K k, int stages, int nslots, bool scal, int &rb, RingGeom &rg, size_t &sm, int &grid)
-    {
-        rb = 128 / T;
-        rg.kp = ring_kp(g.nkxc, T);
-        rg.seg = (unsigned)(sizeof(cplx<R>) * ((g.nkxc + 1) / 2 * 2));
-        rg.stages = stages;
-        for (;;) {
-            sm = tma_smem<R, T, E>(rb, rg, nslots, scal);
-            if (sm <= (size_t)smem_optin || rb * T <= 32) break;
-            rb /= 2;
-        }
-        if (sm > (size_t)smem_optin) return false;
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, rb * T, sm);
-        if (per_sm < 1) return false;
-        const int nbatch = (g.ny * g.nz + rb - 1) / rb;
-        grid = std::min(nbatch, per_sm * num_sms);
-        return true;
-    }
-
     // fast phase-A x pass (3-D); uonly: u only (relaxation finish)
     void xa_launch(int nin, int nout, const PWA<R> &pw, bool grad, bool uonly, const char *name, int nreal)
     {
@@ -658,29 +659,26 @@ public:
                 const int nt = x_threads<T, E>(np, sm);
                 set_smem(k, sm);
                 const int rb = nt / T;
-                launch(name, xbytes(nin, nout, nreal), [&] { k<<<(nrows + rb - 1) / rb, nt, sm, st>>>(g, a, twx, pw); });
+                launch(name, xbytes(nin, nout, nreal), [&] { k<<<(nrows + rb - 1) / rb, nt, sm, st>>>(g, a, tpx, pw); });
             };
-            auto go_tma = [&](auto k, int np) -> bool {
-                int rb, grid;
-                RingGeom rg;
-                size_t sm;
-                if (!tma_config<T, E>(k, np + 1, np, true, rb, rg, sm, grid)) return false;
-                PairList pl;
-                pl.n = np;
-                for (int p = 0; p < np; ++p) {
-                    pl.fa[p] = (signed char)(2 * p);
-                    pl.fb[p] = (signed char)(2 * p + 1 < nin ? 2 * p + 1 : -1);
-                }
-                launch(name, xbytes(nin, nout, nreal),
-                       [&] { k<<<grid, rb * T, sm, st>>>(g, a, twx, pw, rb, rg, pl); });
-                return true;
+            auto go_regs = [&](auto k) {
+                const int nt = 256 / T * T;
+                const size_t sm = xstaged_smem<R, T, E>(nt, 0);
+                set_smem(k, sm);
+                const int rb = nt / T;
+                launch(name, xbytes(nin, nout, nreal), [&] { k<<<(nrows + rb - 1) / rb, nt, sm, st>>>(g, a, tpx, pw); });
             };
-            if (uonly) {
-                if (!(tma_x && go_tma(xa_tma<R, T, E, false, true>, 2))) go(xa_fast<R, T, E, 3, false, true>, 2);
+            const bool no_fd = !ph.has_tf && !ph.has_grad;
+            if (staged_x && uonly) {
+                go_regs(xa_regs<R, T, E, true>);
+            } else if (staged_x && !grad && no_fd) {
+                go_regs(xa_regs<R, T, E, false>);
+            } else if (uonly) {
+                go(xa_fast<R, T, E, 3, false, true>, 2);
             } else if (grad) {
-                if (!(tma_x && go_tma(xa_tma<R, T, E, true, false>, 4))) go(xa_fast<R, T, E, 3, true, false>, 4);
+                go(xa_fast<R, T, E, 3, true, false>, 4);
             } else {
-                if (!(tma_x && go_tma(xa_tma<R, T, E, false, false>, 2))) go(xa_fast<R, T, E, 3, false, false>, 2);
+                go(xa_fast<R, T, E, 3, false, false>, 2);
             }
         });
     }
@@ -696,35 +694,30 @@ public:
                 const int nt = x_threads<T, E>(0, sm);
                 set_smem(k, sm);
                 const int rb = nt / T;
-                launch("xpass_b", xbytes(nin, nout, nreal), [&] { k<<<(nrows + rb - 1) / rb, nt, sm, st>>>(g, a, twx, pw); });
+                launch("xpass_b", xbytes(nin, nout, nreal), [&] { k<<<(nrows + rb - 1) / rb, nt, sm, st>>>(g, a, tpx, pw); });
             };
-            auto go_tma = [&](auto k) -> bool {
-                int rb, grid;
-                RingGeom rg;
-                size_t sm;
-                if (!tma_config<T, E>(k, 4, 0, false, rb, rg, sm, grid)) return false;
-                PairList pl;
-                int np = 0;
-                for (int i = 0; i < nm; i += 2) {
-                    pl.fa[np] = (signed char)i;
-                    pl.fb[np] = (signed char)(i + 1 < nm ? i + 1 : -1);
-                    ++np;
+            auto go_rows = [&](auto k, int nreal_rows) {
+                int nt = 256 / T * T;
+                size_t sm = xstaged_smem<R, T, E>(nt, nreal_rows);
+                while (sm > 110 * 1024 && nt > T) {
+                    nt /= 2;
+                    sm = xstaged_smem<R, T, E>(nt, nreal_rows);
                 }
-                if (ph.evolve)
-                    for (int q = 0; q < 3 * nm; ++q) {
-                        pl.fa[np] = (signed char)(nm + 2 * q);
-                        pl.fb[np] = (signed char)(nm + 2 * q + 1);
-                        ++np;
-                    }
-                pl.n = np;
-                launch("xpass_b", xbytes(nin, nout, nreal),
-                       [&] { k<<<grid, rb * T, sm, st>>>(g, a, twx, pw, rb, rg, pl); });
-                return true;
+                set_smem(k, sm);
+                const int rb = nt / T;
+                launch("xpass_b", xbytes(nin, nout, nreal), [&] { k<<<(nrows + rb - 1) / rb, nt, sm, st>>>(g, a, tpx, pw); });
             };
-            if (ph.evolve) {
-                if (!(tma_x && go_tma(xb_tma<R, T, E, true>))) go(xb_fast<R, T, E, 3, true>);
+            const bool ext = ph.ext_active != 0;
+            if (staged_x && ph.evolve) {
+                if (ext) go_rows(xb_rows<R, T, E, true, true>, 4);
+                else go_rows(xb_rows<R, T, E, true, false>, 4);
+            } else if (staged_x) {
+                if (ext) go_rows(xb_rows<R, T, E, false, true>, 1);
+                else go_rows(xb_rows<R, T, E, false, false>, 1);
+            } else if (ph.evolve) {
+                go(xb_fast<R, T, E, 3, true>);
             } else {
-                if (!(tma_x && go_tma(xb_tma<R, T, E, false>))) go(xb_fast<R, T, E, 3, false>);
+                go(xb_fast<R, T, E, 3, false>);
             }
         });
     }
@@ -740,7 +733,7 @@ public:
                 const int nt = x_threads<T, E>(0, sm);
                 set_smem(k, sm);
                 const int rb = nt / T;
-                launch(name, xbytes(nin, nout, nin + nout), [&] { k<<<(nrows + rb - 1) / rb, nt, sm, st>>>(g, a, twx, dst, src); });
+                launch(name, xbytes(nin, nout, nin + nout), [&] { k<<<(nrows + rb - 1) / rb, nt, sm, st>>>(g, a, tpx, dst, src); });
             };
             if (nin > 0) go(xio_fast<R, T, E, true>);
             else go(xio_fast<R, T, E, false>);
