@@ -35,6 +35,8 @@ UNIT = "cell-steps/s"
 # algorithmic bytes per cell-step of the minimal exact transform schedule,
 # Maxwell ions: 3 stages x (8 B x 44 transforms + 16 B x 10 state fields), FP32
 STEP_BYTES_FP32 = 3 * (8 * 44 + 16 * 10)
+# Newtonian ions: 3 stages x (8 B x 20 transforms + 16 B x 4 state fields)
+STEP_BYTES_FP32_NEWTONIAN = 3 * (8 * 20 + 16 * 4)
 
 
 def workload_params(hg, n, precision, L=64.0):
@@ -201,6 +203,125 @@ def run_reference(args):
     return 0
 
 
+# transforms per RK3 step of the Maxwell ion step: the minimal exact schedule
+# this library runs (per stage 24 inverse + 20 forward) and the reference's
+# literal schedule (369 3-D transforms per step)
+MIN_C2R, MIN_R2C = 3 * 24, 3 * 20
+LITERAL_TRANSFORMS = 369
+
+
+def cufft_comparator(torch, dev, n):
+    """cuFFT (through torch.fft) timed on the same grid, as a comparator only:
+    the transforms alone, no physics.  FP32 at the minimal schedule's count,
+    FP64 at the reference's literal count (split evenly between r2c and c2r)."""
+    out = {}
+    for dt, name in ((torch.float32, "fp32"), (torch.float64, "fp64")):
+        x = torch.randn((n, n, n), dtype=dt, device=dev)
+        xh = torch.fft.rfftn(x)
+        for _ in range(3):
+            torch.fft.irfftn(torch.fft.rfftn(x), s=x.shape)
+        reps = 10
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        torch.cuda.synchronize(dev)
+        e[0].record()
+        for _ in range(reps):
+            torch.fft.rfftn(x)
+        e[1].record()
+        for _ in range(reps):
+            torch.fft.irfftn(xh, s=x.shape)
+        e[2].record()
+        torch.cuda.synchronize(dev)
+        r2c = e[0].elapsed_time(e[1]) / reps
+        c2r = e[1].elapsed_time(e[2]) / reps
+        out[name] = {"r2c_ms": r2c, "c2r_ms": c2r}
+        del x, xh
+    f32, f64 = out["fp32"], out["fp64"]
+    out["fp32_min_schedule_ms_per_step"] = MIN_C2R * f32["c2r_ms"] + MIN_R2C * f32["r2c_ms"]
+    out["fp64_literal_schedule_ms_per_step"] = LITERAL_TRANSFORMS / 2 * (f64["c2r_ms"] + f64["r2c_ms"])
+    out["note"] = ("torch.fft (cuFFT) transforms only, full half spectrum, no band pruning, no physics; "
+                   "a lower bound on a cuFFT-based step at each schedule")
+    return out
+
+
+def batch_members(hg, count, seed=2025):
+    """The ensemble workload: grids from {32,48,64,96,128}^3 (dx of the
+    32^3, L = 20 a case), Gamma log-uniform in [1, 100], kappa uniform in
+    [0.5, 3], Newtonian / Maxwell 50/50, one Fourier mode from the lowest
+    four shells at amplitude 1e-3, FP32 fields."""
+    rng = np.random.default_rng(seed)
+    shells = [m for m in np.ndindex(5, 5, 5) if 1 <= sum(x * x for x in m) <= 4]
+    out = []
+    for _ in range(count):
+        n = int(rng.choice([32, 48, 64, 96, 128]))
+        L = 20.0 * n / 32.0
+        gamma = float(10 ** rng.uniform(0.0, 2.0))
+        kappa = float(rng.uniform(0.5, 3.0))
+        maxwell = bool(rng.integers(0, 2))
+        mode = shells[int(rng.integers(0, len(shells)))]
+        kw = dict(kind="ion", gamma=gamma, kappa=kappa, nx=n, ny=n, nz=n, lx=L, ly=L, lz=L,
+                  transport="yukawa_fit", hnc_nr=4096, hnc_rmax=80.0, cfl=0.4, dt=0.0, gpu_precision="fp32",
+                  closure="maxwell" if maxwell else "newtonian", ic="mode", ic_amplitude=1e-3,
+                  ic_mode=tuple(int(x) for x in mode))
+        if maxwell:
+            kw["tau_model"] = "ichimaru"
+        out.append(kw)
+    return out
+
+
+def run_batch_leg(torch, hg, count, steps, warmup, dev):
+    """The ensemble advanced by one graph launch per step; cell-steps/s over
+    all members, with the roofline of the minimal schedule's bytes."""
+    members = batch_members(hg, count)
+    t0 = time.perf_counter()
+    b = hg.Batch([hg.default_params(**kw) for kw in members], device=dev)
+    setup_s = time.perf_counter() - t0
+    cells = 0.0
+    bytes_step = 0.0
+    for kw, m in zip(members, b.members):
+        m.set_initial_condition("mode", kw["ic_amplitude"], kw["ic_mode"])
+        m.compute_dt()
+        c = float(kw["nx"]) ** 3
+        cells += c
+        bytes_step += c * (STEP_BYTES_FP32 if kw["closure"] == "maxwell" else STEP_BYTES_FP32_NEWTONIAN)
+    b.advance(warmup)
+    stream = torch.cuda.ExternalStream(b.stream_ptr(), device=dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    l0 = b.launch_count()
+    e0.record(stream)
+    b.advance(steps)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1)
+    launches = b.launch_count() - l0
+    # per-step device times: p50 / p99
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    evs[0].record(stream)
+    for i in range(steps):
+        b.advance(1)
+        evs[i + 1].record(stream)
+    torch.cuda.synchronize(dev)
+    per = np.array([evs[i].elapsed_time(evs[i + 1]) for i in range(steps)])
+    peak, _ = measured_peak()
+    achieved = bytes_step * steps / (ms * 1e-3) / 1e9
+    sizes = {}
+    for kw in members:
+        sizes[kw["nx"]] = sizes.get(kw["nx"], 0) + 1
+    out = {"workload": "ensemble of %d ion runs, grids {32,48,64,96,128}^3, Gamma log-uniform [1,100], "
+                       "kappa uniform [0.5,3], Newtonian/Maxwell 50/50, one mode amplitude 1e-3, FP32" % count,
+           "members": count, "members_per_grid": {str(k): v for k, v in sorted(sizes.items())},
+           "maxwell_members": sum(1 for kw in members if kw["closure"] == "maxwell"),
+           "cells": cells, "value": cells * steps / (ms * 1e-3), "unit": UNIT, "steps": steps,
+           "ms_per_step": ms / steps, "step_ms_p50": float(np.percentile(per, 50)),
+           "step_ms_p99": float(np.percentile(per, 99)), "gpu_launches": int(launches),
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "bytes_per_step": bytes_step},
+           "setup_s": setup_s}
+    b.close()
+    return out
+
+
 def structure_for_workload(hg, device):
     m = hg.Model(workload_params(hg, 8, "fp64"), device=device)
     k, c = m.structure()
@@ -219,15 +340,27 @@ def main():
     ap.add_argument("--ref-n", type=int, default=64)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-plain leg")
+    ap.add_argument("--no-cufft", action="store_true", help="skip the cuFFT comparator")
     ap.add_argument("--quick", action="store_true",
                     help="setup, warm-up and the timed steps only (for profiler captures)")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--batch-members", type=int, default=0,
+                    help="also time the ensemble workload with this many members (0: skip)")
+    ap.add_argument("--workload", default="maxwell256", choices=["maxwell256", "batch"],
+                    help="batch: time only the ensemble workload (256 members unless --batch-members)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
 
     import torch
     import hydft_b200 as hg
+
+    if args.workload == "batch":
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        res = run_batch_leg(torch, hg, args.batch_members or 256, args.steps, args.warmup,
+                            int(os.environ.get("LOCAL_RANK", "0")))
+        print(json.dumps(res), flush=True)
+        return 0
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -313,6 +446,21 @@ def main():
                for k, v in prof.items()}
 
     extra = {}
+    # per-step device times (one graph replay each, CUDA events between steps)
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    torch.cuda.synchronize(dev)
+    evs[0].record(stream)
+    for i in range(args.steps):
+        m32.advance(1)
+        evs[i + 1].record(stream)
+    torch.cuda.synchronize(dev)
+    per_step = np.array([evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)])
+    extra["step_ms"] = {"p50": float(np.percentile(per_step, 50)), "p99": float(np.percentile(per_step, 99)),
+                        "min": float(per_step.min()), "max": float(per_step.max()), "n": int(args.steps)}
+    if not args.no_cufft:
+        extra["cufft_comparator"] = cufft_comparator(torch, dev, n)
+    if args.batch_members > 0:
+        extra["batch"] = run_batch_leg(torch, hg, args.batch_members, max(3, args.steps // 3), args.warmup, dev)
     # FP64-plain leg and the FP32 field error against it
     if not args.no_fp64:
         m64 = hg.Model(workload_params(hg, n, "fp64"), structure=st, device=dev)

@@ -10,18 +10,10 @@
 #include <vector>
 
 #include "../../include/hydft_gpu.h"
-#include "setup.hpp"
+#include "handle.hpp"
 #include "setup_gpu.hpp"
-#include "solver.hpp"
 
 using namespace hydft;
-
-struct hydft_gpu {
-    ModelHost mh;
-    SolverBase *s = nullptr;
-    int device = 0;
-    std::string err;
-};
 
 static thread_local std::string g_create_err;
 
@@ -92,7 +84,7 @@ int hydft_gpu_create(const hydft_params *p, const hydft_structure *st, int devic
 
 void hydft_gpu_destroy(hydft_gpu *h)
 {
-    if (!h) return;
+    if (!h || h->owned_by_batch) return;
     if (h->s) {
         cudaSetDevice(h->device);
         delete h->s;

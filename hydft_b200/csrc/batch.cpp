@@ -1,0 +1,288 @@
+// Ensembles: many independent simulations (different grids, Gamma, kappa,
+// closures) advanced together by one CUDA graph launch per step.
+//
+// Each member is a full hydft_gpu handle with its own device state, work
+// buffers and stream.  The ensemble captures one RK3 step of every member
+// into a single graph: a fork event on the ensemble's root stream, each
+// member's step kernels on its own stream, and a join back to the root, so
+// the members are independent branches that the GPU runs concurrently (a
+// 32^3 member alone cannot fill 148 SMs; hundreds of them side by side
+// can).  Replaying the graph advances every member by one step with one
+// launch.  The reference runs one model_t per process (src/hydft.f90:41-51,
+// the loop every member follows); this grouping has no counterpart there.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/hydft_gpu.h"
+#include "handle.hpp"
+
+using namespace hydft;
+
+struct hydft_batch {
+    std::vector<hydft_gpu *> m;
+    int device = 0;
+    cudaStream_t root = nullptr;
+    cudaEvent_t fork = nullptr, done = nullptr;
+    std::vector<cudaEvent_t> join;
+    cudaGraphExec_t gexec = nullptr;
+    std::vector<int64_t> gens;           // member graph generations at capture
+    std::vector<int64_t> step_launches;  // kernels of one member step
+    unsigned *hstat = nullptr;           // pinned status words, one per member
+    int failed = -1;
+    std::string err;
+};
+
+namespace {
+
+struct CachedStructure {
+    std::vector<double> k, c;
+    double u_ex = 0, du_dgamma = 0;
+    int has_energy = 0;
+};
+
+// members whose HNC inputs agree share one solve
+std::string hnc_key(const hydft_params &p)
+{
+    char buf[512];
+    std::snprintf(buf, sizeof buf, "%s|%.17g|%.17g|%.17g|%.17g|%.17g|%d|%.17g|%.17g|%.17g|%d|%s|%s", p.kind, p.gamma,
+                  p.kappa, p.rs, p.theta, p.mass, p.hnc_nr, p.hnc_rmax, p.hnc_tol, p.hnc_mix, p.hnc_maxiter,
+                  p.structure, p.structure_kind);
+    return buf;
+}
+
+int fail(hydft_batch *b, int rc, const std::string &msg)
+{
+    b->err = msg;
+    return rc;
+}
+
+void destroy_member(hydft_gpu *h)
+{
+    if (!h) return;
+    if (h->s) {
+        cudaSetDevice(h->device);
+        delete h->s;
+    }
+    delete h;
+}
+
+void drop_graph(hydft_batch *b)
+{
+    if (b->gexec) cudaGraphExecDestroy(b->gexec);
+    b->gexec = nullptr;
+}
+
+// one graph: fork -> every member's step on its stream -> join
+int capture(hydft_batch *b)
+{
+    drop_graph(b);
+    const size_t n = b->m.size();
+    std::vector<int64_t> before(n);
+    for (size_t i = 0; i < n; ++i) before[i] = b->m[i]->s->launches;
+    cudaError_t e = cudaStreamBeginCapture(b->root, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return fail(b, HYDFT_ERR_CUDA, std::string("begin capture: ") + cudaGetErrorString(e));
+    cudaEventRecord(b->fork, b->root);
+    for (size_t i = 0; i < n; ++i) {
+        cudaStream_t s = static_cast<cudaStream_t>(b->m[i]->s->stream());
+        cudaStreamWaitEvent(s, b->fork, 0);
+        b->m[i]->s->enqueue_steps(1);
+        cudaEventRecord(b->join[i], s);
+        cudaStreamWaitEvent(b->root, b->join[i], 0);
+    }
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(b->root, &g);
+    if (e != cudaSuccess) return fail(b, HYDFT_ERR_CUDA, std::string("end capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&b->gexec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(b, HYDFT_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    for (size_t i = 0; i < n; ++i) {
+        b->step_launches[i] = b->m[i]->s->launches - before[i];
+        b->m[i]->s->launches = before[i];
+        b->gens[i] = b->m[i]->s->graph_gen;
+    }
+    return HYDFT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hydft_batch_create(int n, const hydft_params *params, const hydft_structure *structures, int device,
+                       hydft_batch **out)
+{
+    if (n < 1 || !params || !out) return HYDFT_ERR_BAD_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        set_thread_error("no CUDA device available (the solver has no CPU path)");
+        return HYDFT_ERR_CUDA;
+    }
+    cudaSetDevice(device);
+    auto b = std::make_unique<hydft_batch>();
+    b->device = device;
+    std::map<std::string, CachedStructure> cache;
+    auto cleanup = [&]() {
+        for (auto *h : b->m) destroy_member(h);
+        b->m.clear();
+    };
+    for (int i = 0; i < n; ++i) {
+        const hydft_params &p = params[i];
+        hydft_structure st{};
+        const hydft_structure *sp = nullptr;
+        const bool given = structures && structures[i].n > 0;
+        const std::string key = hnc_key(p);
+        const bool hnc = std::string(p.structure) == "hnc";
+        if (given) {
+            sp = &structures[i];
+        } else if (hnc && cache.count(key)) {
+            const CachedStructure &c = cache[key];
+            st.n = (int)c.k.size();
+            st.k = c.k.data();
+            st.c = c.c.data();
+            st.u_ex = c.u_ex;
+            st.du_dgamma = c.du_dgamma;
+            st.has_energy = c.has_energy;
+            sp = &st;
+        }
+        hydft_gpu *h = nullptr;
+        int rc = hydft_gpu_create(&p, sp, device, &h);
+        if (rc) {
+            const std::string msg = "member " + std::to_string(i) + ": " + hydft_gpu_create_error();
+            cleanup();
+            set_thread_error(msg);
+            return rc;
+        }
+        h->owned_by_batch = true;
+        b->m.push_back(h);
+        if (!given && hnc && !cache.count(key) && h->mh.has_st) {
+            CachedStructure c;
+            c.k = h->mh.st_k;
+            c.c = h->mh.st_c;
+            c.u_ex = h->mh.u_ex;
+            c.du_dgamma = h->mh.du_dgamma;
+            c.has_energy = h->mh.has_energy ? 1 : 0;
+            cache[key] = std::move(c);
+        }
+    }
+    cudaSetDevice(device);
+    if (cudaStreamCreateWithFlags(&b->root, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) != cudaSuccess ||
+        cudaMallocHost(&b->hstat, sizeof(unsigned) * n) != cudaSuccess) {
+        cleanup();
+        set_thread_error("ensemble: stream, event or pinned buffer creation failed");
+        return HYDFT_ERR_CUDA;
+    }
+    b->join.resize(n);
+    for (int i = 0; i < n; ++i)
+        if (cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming) != cudaSuccess) {
+            cleanup();
+            set_thread_error("ensemble: event creation failed");
+            return HYDFT_ERR_CUDA;
+        }
+    b->gens.assign(n, -1);
+    b->step_launches.assign(n, 0);
+    *out = b.release();
+    return HYDFT_OK;
+}
+
+void hydft_batch_destroy(hydft_batch *b)
+{
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->root) cudaStreamSynchronize(b->root);
+    drop_graph(b);
+    for (auto *h : b->m) destroy_member(h);
+    for (auto e : b->join)
+        if (e) cudaEventDestroy(e);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->done) cudaEventDestroy(b->done);
+    if (b->root) cudaStreamDestroy(b->root);
+    if (b->hstat) cudaFreeHost(b->hstat);
+    delete b;
+}
+
+int hydft_batch_size(const hydft_batch *b) { return b ? (int)b->m.size() : 0; }
+
+int hydft_batch_member(hydft_batch *b, int i, hydft_gpu **member)
+{
+    if (!b || !member || i < 0 || i >= (int)b->m.size()) return HYDFT_ERR_BAD_ARG;
+    *member = b->m[i];
+    return HYDFT_OK;
+}
+
+const char *hydft_batch_last_error(const hydft_batch *b) { return b ? b->err.c_str() : ""; }
+
+int hydft_batch_failed_member(const hydft_batch *b) { return b ? b->failed : -1; }
+
+int hydft_batch_advance(hydft_batch *b, int nsteps)
+{
+    if (!b || nsteps < 0) return HYDFT_ERR_BAD_ARG;
+    if (nsteps == 0) return HYDFT_OK;
+    cudaSetDevice(b->device);
+    const size_t n = b->m.size();
+    b->failed = -1;
+    for (size_t i = 0; i < n; ++i) {
+        double t, dt;
+        int64_t s;
+        b->m[i]->s->get_time(&t, &dt, &s);
+        if (!(dt > 0.0)) {
+            b->failed = (int)i;
+            return fail(b, HYDFT_ERR_BAD_ARG, "member " + std::to_string(i) + ": dt is not set (call compute_dt)");
+        }
+    }
+    bool stale = !b->gexec;
+    for (size_t i = 0; i < n && !stale; ++i) stale = b->gens[i] != b->m[i]->s->graph_gen;
+    if (stale)
+        if (int rc = capture(b)) return rc;
+    // the graph starts after whatever the members' own streams hold
+    for (size_t i = 0; i < n; ++i) {
+        cudaStream_t s = static_cast<cudaStream_t>(b->m[i]->s->stream());
+        cudaEventRecord(b->join[i], s);
+        cudaStreamWaitEvent(b->root, b->join[i], 0);
+    }
+    for (int k = 0; k < nsteps; ++k) {
+        cudaError_t e = cudaGraphLaunch(b->gexec, b->root);
+        if (e != cudaSuccess) return fail(b, HYDFT_ERR_CUDA, std::string("graph launch: ") + cudaGetErrorString(e));
+    }
+    for (size_t i = 0; i < n; ++i) {
+        b->m[i]->s->launches += b->step_launches[i] * nsteps;
+        cudaMemcpyAsync(b->hstat + i, b->m[i]->s->status_word(), sizeof(unsigned), cudaMemcpyDeviceToHost, b->root);
+    }
+    // later work on the members' streams follows the graph
+    cudaEventRecord(b->done, b->root);
+    for (size_t i = 0; i < n; ++i)
+        cudaStreamWaitEvent(static_cast<cudaStream_t>(b->m[i]->s->stream()), b->done, 0);
+    cudaError_t e = cudaStreamSynchronize(b->root);
+    if (e != cudaSuccess) return fail(b, HYDFT_ERR_CUDA, std::string("ensemble step: ") + cudaGetErrorString(e));
+    for (size_t i = 0; i < n; ++i) {
+        // time and step count live on the device and advanced with the graph
+        b->m[i]->s->mark_advanced();
+        if (b->hstat[i]) {
+            const int rc = b->m[i]->s->take_status(b->hstat[i]);
+            if (rc) {
+                b->failed = (int)i;
+                return fail(b, rc, "member " + std::to_string(i) + ": " + b->m[i]->s->err);
+            }
+        }
+    }
+    return HYDFT_OK;
+}
+
+int64_t hydft_batch_launch_count(const hydft_batch *b)
+{
+    if (!b) return 0;
+    int64_t t = 0;
+    for (auto *h : b->m) t += h->s->launches;
+    return t;
+}
+
+void *hydft_batch_stream(const hydft_batch *b) { return b ? (void *)b->root : nullptr; }
+
+}  // extern "C"

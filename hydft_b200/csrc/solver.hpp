@@ -62,7 +62,19 @@ public:
     virtual int profile(int nsteps, std::vector<KernelStat> &out) = 0;
     // the host-side setup constants in use
     virtual const SolverSetup &setup() const = 0;
+    // Enqueues k RK3 steps on this solver's stream without capturing,
+    // launching a graph or synchronising (an ensemble captures the steps of
+    // many solvers into one graph through this call).
+    virtual void enqueue_steps(int k) = 0;
+    // records that steps enqueued earlier (a replayed ensemble graph) ran
+    virtual void mark_advanced() = 0;
+    // device address of the status word the step kernels set (ST_* bits)
+    virtual const unsigned *status_word() const = 0;
+    // turns status bits read from status_word() into an error code and
+    // message, and clears the device word; 0 if stv is 0
+    virtual int take_status(unsigned stv) = 0;
     int64_t launches = 0;
+    int64_t graph_gen = 0;   // bumped when values baked into captured steps change
     std::string err;
 };
 

@@ -281,6 +281,7 @@ public:
     {
         S.ext_omega = w;
         ph.ext_omega = w;
+        ++graph_gen;
         if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
         if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
     }
@@ -954,6 +955,11 @@ public:
         unsigned stv = 0;
         CK(cudaMemcpyAsync(&stv, &ctrl->status, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        return take_status(stv);
+    }
+
+    int take_status(unsigned stv) override
+    {
         if (stv) {
             CK(cudaMemsetAsync(&ctrl->status, 0, sizeof(unsigned), st));
             if (stv & ST_NONFINITE) { err = "state is not finite (NaN or Inf)"; return HYDFT_E_NONFINITE; }
@@ -964,6 +970,16 @@ public:
         }
         return 0;
     }
+
+    const unsigned *status_word() const override { return &ctrl->status; }
+
+    void enqueue_steps(int k) override
+    {
+        for (int i = 0; i < k; ++i) one_step();
+        if (k > 0) host_pending = ph.evolve != 0;
+    }
+
+    void mark_advanced() override { host_pending = ph.evolve != 0; }
 
     int64_t step_launches = 0;
 

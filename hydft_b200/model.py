@@ -116,6 +116,18 @@ def lib():
         L.hydft_gpu_fourier_bessel.argtypes = [_P, _P, _I, _D, _I, _I]
         L.hydft_gpu_fd_table.argtypes = [_I, _P, C.POINTER(_I)]
         L.hydft_gpu_fd_alpha.argtypes = [_I, _P, _P, _I]
+        L.hydft_batch_create.argtypes = [_I, _P, _P, _I, C.POINTER(_P)]
+        L.hydft_batch_destroy.argtypes = [_P]
+        L.hydft_batch_size.argtypes = [_P]
+        L.hydft_batch_member.argtypes = [_P, _I, C.POINTER(_P)]
+        L.hydft_batch_advance.argtypes = [_P, _I]
+        L.hydft_batch_last_error.restype = C.c_char_p
+        L.hydft_batch_last_error.argtypes = [_P]
+        L.hydft_batch_failed_member.argtypes = [_P]
+        L.hydft_batch_launch_count.restype = C.c_int64
+        L.hydft_batch_launch_count.argtypes = [_P]
+        L.hydft_batch_stream.restype = _P
+        L.hydft_batch_stream.argtypes = [_P]
         _lib = L
     return _lib
 
@@ -178,7 +190,23 @@ class Model:
         self.shape = (p.nz, p.ny, p.nx)
         self.has_pi = bool(self.scalar("evolve"))
 
+    @classmethod
+    def _member(cls, h, p, owner):
+        """A view of an ensemble member (the ensemble owns the handle)."""
+        m = cls.__new__(cls)
+        m._keep = None
+        m.h = h
+        m.p = p
+        m._owner = owner
+        m.nx, m.ny, m.nz = p.nx, p.ny, p.nz
+        m.shape = (p.nz, p.ny, p.nx)
+        m.has_pi = bool(m.scalar("evolve"))
+        return m
+
     def close(self):
+        if getattr(self, "_owner", None) is not None:
+            self.h = None
+            return
         if getattr(self, "h", None):
             lib().hydft_gpu_destroy(self.h)
             self.h = None
@@ -364,3 +392,72 @@ def fd_alpha(y, device=0):
     if rc:
         raise HydftError(rc, lib().hydft_gpu_create_error().decode())
     return a
+
+
+class Batch:
+    """An ensemble of independent models advanced by one graph launch per
+    step (hydft_batch_* in include/hydft_gpu.h).  `members[i]` is a Model
+    view of member i for the single-model calls."""
+
+    def __init__(self, params, structures=None, device=0):
+        L = lib()
+        n = len(params)
+        arr = (Params * n)(*params)
+        sts = None
+        self._keep = []
+        if structures is not None:
+            sts = (Structure * n)()
+            for i, st in enumerate(structures):
+                if st is None:
+                    sts[i].n = 0
+                    continue
+                k = np.ascontiguousarray(st["k"], dtype=np.float64)
+                c = np.ascontiguousarray(st["c"], dtype=np.float64)
+                self._keep.append((k, c))
+                sts[i] = Structure(k.size, k.ctypes.data_as(C.POINTER(_D)), c.ctypes.data_as(C.POINTER(_D)),
+                                   st.get("u_ex", 0.0), st.get("du_dgamma", 0.0),
+                                   1 if st.get("has_energy", True) else 0)
+        b = _P()
+        rc = L.hydft_batch_create(n, C.cast(arr, _P), C.cast(sts, _P) if sts is not None else None, device,
+                                  C.byref(b))
+        if rc:
+            raise HydftError(rc, L.hydft_gpu_create_error().decode())
+        self.b = b
+        self.params = list(params)
+        self.members = []
+        for i in range(n):
+            h = _P()
+            self._check(L.hydft_batch_member(b, i, C.byref(h)))
+            self.members.append(Model._member(h, self.params[i], self))
+
+    def _check(self, rc):
+        if rc:
+            raise HydftError(rc, lib().hydft_batch_last_error(self.b).decode())
+
+    def __len__(self):
+        return len(self.members)
+
+    def advance(self, nsteps=1):
+        self._check(lib().hydft_batch_advance(self.b, int(nsteps)))
+
+    def failed_member(self):
+        return lib().hydft_batch_failed_member(self.b)
+
+    def launch_count(self):
+        return lib().hydft_batch_launch_count(self.b)
+
+    def stream_ptr(self):
+        return lib().hydft_batch_stream(self.b)
+
+    def close(self):
+        if getattr(self, "b", None):
+            for m in self.members:
+                m.h = None
+            lib().hydft_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

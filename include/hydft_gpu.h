@@ -249,6 +249,38 @@ int hydft_gpu_fd_table(int device, double *out, int *ntab);
  * on the GPU for n host values. */
 int hydft_gpu_fd_alpha(int device, const double *y, double *alpha, int n);
 
+/*
+ * Ensembles.  The reference runs one model_t per process and steps it in
+ * the driver loop of src/hydft.f90:41-51; an ensemble holds many such
+ * models (each with its own grid, species, Gamma, kappa and closure) on one
+ * GPU and advances all of them by one RK3 step per launch of a single
+ * captured CUDA graph in which every member is an independent branch.
+ *
+ * hydft_batch_create builds n members from params[i] (and structures[i]
+ * when structures != NULL and structures[i].n > 0; members whose HNC
+ * inputs agree share one OZ-HNC solve).  Errors: hydft_gpu_create_error().
+ * hydft_batch_member gives member i as a hydft_gpu handle for every
+ * single-model call (set_state, set_initial_condition, compute_dt,
+ * get_state, budgets, mode, ...); the handle belongs to the ensemble and
+ * hydft_gpu_destroy ignores it.  hydft_batch_advance runs nsteps ensemble
+ * steps (every member at its own dt, which must be set) and then checks
+ * every member's status; on an error hydft_batch_failed_member names the
+ * first failing member and hydft_batch_last_error gives its message.
+ */
+typedef struct hydft_batch hydft_batch;
+int hydft_batch_create(int n, const hydft_params *params, const hydft_structure *structures, int device,
+                       hydft_batch **out);
+void hydft_batch_destroy(hydft_batch *b);
+int hydft_batch_size(const hydft_batch *b);
+int hydft_batch_member(hydft_batch *b, int i, hydft_gpu **member);
+int hydft_batch_advance(hydft_batch *b, int nsteps);
+const char *hydft_batch_last_error(const hydft_batch *b);
+int hydft_batch_failed_member(const hydft_batch *b);
+/* kernels launched for all members so far, and the stream the ensemble
+ * graph runs on (a cudaStream_t) */
+int64_t hydft_batch_launch_count(const hydft_batch *b);
+void *hydft_batch_stream(const hydft_batch *b);
+
 #ifdef __cplusplus
 }
 #endif
