@@ -322,6 +322,85 @@ def run_batch_leg(torch, hg, count, steps, warmup, dev):
     return out
 
 
+# even 2^a 3^b lengths in [32, 256] (the GPU path's FFT lengths)
+SERVE_SIZES = [32, 36, 48, 54, 64, 72, 96, 108, 128, 144, 162, 192, 216, 256]
+
+
+def serve_request(hg, rng, step_scale):
+    """One request of the serving stream: an ion Newtonian (Gamma 10, kappa 1,
+    dx 0.625), ion Maxwell (Gamma 50, kappa 2, Ichimaru tau, dx 0.25) or
+    electron driven (r_s 1, theta 1, dx 0.3125) solve on an N^3 grid drawn
+    uniformly from SERVE_SIZES, 500-5000 RK3 steps, FP32 fields."""
+    n = int(rng.choice(SERVE_SIZES))
+    kind = int(rng.integers(0, 3))
+    steps = max(1, int(round(int(rng.integers(500, 5001)) * step_scale)))
+    common = dict(nx=n, ny=n, nz=n, gpu_precision="fp32", hnc_nr=4096, hnc_rmax=80.0, cfl=0.4, dt=0.0,
+                  ic="mode", ic_amplitude=1e-3, ic_mode=(1, 0, 0))
+    if kind == 0:
+        L = 0.625 * n
+        kw = dict(kind="ion", gamma=10.0, kappa=1.0, transport="yukawa_fit", lx=L, ly=L, lz=L, **common)
+    elif kind == 1:
+        L = 0.25 * n
+        kw = dict(kind="ion", gamma=50.0, kappa=2.0, closure="maxwell", transport="yukawa_fit",
+                  tau_model="ichimaru", lx=L, ly=L, lz=L, **common)
+    else:
+        L = 0.3125 * n
+        kw = dict(kind="electron", rs=1.0, theta=1.0, transport="constant", eta=0.2, vext="driven",
+                  vext_amplitude=1e-4, vext_mode=(3, 0, 0), vext_omega=1.0, lx=L, ly=L, lz=L, **common)
+        kw["ic"] = "uniform"
+    return ("ion_newtonian", "ion_maxwell", "electron_driven")[kind], n, steps, kw
+
+
+def run_serve_leg(hg, dev, rates, per_rate, step_scale, seed=7):
+    """Poisson arrivals at each rate into one continuous-batching server;
+    latency (submit to completion) p50/p99 and throughput per rate."""
+    rng = np.random.default_rng(seed)
+    srv = hg.Server(device=dev, max_slots=64, chunk_steps=25)
+    out = {"workload": "serving stream: Poisson arrivals; ion Newtonian / ion Maxwell / electron driven solves on "
+                       "N^3, N uniform over %s, 500-5000 RK3 steps x %g, FP32" % (SERVE_SIZES, step_scale),
+           "per_rate": per_rate, "rates": []}
+    try:
+        for lam in rates:
+            reqs = [serve_request(hg, rng, step_scale) for _ in range(per_rate)]
+            gaps = rng.exponential(1.0 / lam, size=per_rate)
+            ids = []
+            t0 = time.perf_counter()
+            at = 0.0
+            for (name, n, steps, kw), gap in zip(reqs, gaps):
+                at += gap
+                delay = at - (time.perf_counter() - t0)
+                if delay > 0:
+                    time.sleep(delay)
+                ids.append(srv.submit(hg.default_params(**kw), steps))
+            lat, lat_nosetup, work, first, last = [], [], 0.0, None, None
+            failed = 0
+            for rid, (name, n, steps, kw) in zip(ids, reqs):
+                srv.wait(rid)
+                try:
+                    info, _ = srv.result(rid)
+                except hg.HydftError:
+                    failed += 1
+                    continue
+                lat.append(info["t_done"] - info["t_submit"])
+                lat_nosetup.append(info["t_done"] - info["t_submit"] - (info["t_start"] - info["t_admit"]))
+                work += float(n) ** 3 * steps
+                first = info["t_submit"] if first is None else min(first, info["t_submit"])
+                last = info["t_done"] if last is None else max(last, info["t_done"])
+            st = srv.stats()
+            out["rates"].append({
+                "lambda_per_s": lam, "requests": per_rate, "failed": failed,
+                "latency_s_p50": float(np.percentile(lat, 50)) if lat else None,
+                "latency_s_p99": float(np.percentile(lat, 99)) if lat else None,
+                "latency_excl_setup_s_p50": float(np.percentile(lat_nosetup, 50)) if lat else None,
+                "latency_excl_setup_s_p99": float(np.percentile(lat_nosetup, 99)) if lat else None,
+                "throughput_cell_steps_per_s": work / (last - first) if lat else None,
+                "throughput_req_per_s": len(lat) / (last - first) if lat else None,
+                "max_requests_resident": st["max_holding"]})
+    finally:
+        srv.close()
+    return out
+
+
 def structure_for_workload(hg, device):
     m = hg.Model(workload_params(hg, 8, "fp64"), device=device)
     k, c = m.structure()
@@ -346,8 +425,12 @@ def main():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--batch-members", type=int, default=0,
                     help="also time the ensemble workload with this many members (0: skip)")
-    ap.add_argument("--workload", default="maxwell256", choices=["maxwell256", "batch"],
-                    help="batch: time only the ensemble workload (256 members unless --batch-members)")
+    ap.add_argument("--workload", default="maxwell256", choices=["maxwell256", "batch", "serve"],
+                    help="batch: time only the ensemble workload (256 members unless --batch-members); "
+                         "serve: the serving stream at --rates")
+    ap.add_argument("--rates", default="10,30,100,300,1000", help="serving arrival rates (requests/s)")
+    ap.add_argument("--per-rate", type=int, default=6, help="serving requests per rate")
+    ap.add_argument("--step-scale", type=float, default=1.0, help="serving steps scale (1: 500-5000)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -355,6 +438,12 @@ def main():
     import torch
     import hydft_b200 as hg
 
+    if args.workload == "serve":
+        dev = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(dev)
+        res = run_serve_leg(hg, dev, [float(x) for x in args.rates.split(",")], args.per_rate, args.step_scale)
+        print(json.dumps(res), flush=True)
+        return 0
     if args.workload == "batch":
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         res = run_batch_leg(torch, hg, args.batch_members or 256, args.steps, args.warmup,

@@ -82,6 +82,13 @@ int hydft_gpu_create(const hydft_params *p, const hydft_structure *st, int devic
     return HYDFT_OK;
 }
 
+int hydft_gpu_footprint(const hydft_params *p, double *bytes)
+{
+    if (!p || !bytes) return HYDFT_ERR_BAD_ARG;
+    *bytes = footprint_bytes(p);
+    return *bytes < 0 ? HYDFT_ERR_BAD_ARG : HYDFT_OK;
+}
+
 void hydft_gpu_destroy(hydft_gpu *h)
 {
     if (!h || h->owned_by_batch) return;
@@ -316,6 +323,7 @@ int hydft_gpu_get_scalar(const hydft_gpu *h, const char *name, double *v)
     else if (k == "ndim") *v = m.S.g.ndim;
     else if (k == "evolve") *v = m.evolve ? 1.0 : 0.0;
     else if (k == "precision") *v = m.precision;
+    else if (k == "device_bytes") *v = (double)h->s->device_bytes();
     else if (k == "ext_omega") *v = m.ext_omega;
     else if (k == "hnc_niter") *v = m.hnc_niter;
     else if (k == "wmax") *v = m.wmax;

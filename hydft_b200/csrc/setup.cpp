@@ -366,6 +366,30 @@ static int band_limit(int n, double L, int dealias)
     return M;
 }
 
+double footprint_bytes(const hydft_params *pin)
+{
+    hydft_params p = *pin;
+    params_finalize(&p);
+    if (p.nx < 2 || p.ny < 1 || p.nz < 1) return -1.0;
+    const double b = std::string(p.gpu_precision) == "fp32" ? 4.0 : 8.0, cb = 2.0 * b;
+    const int Mx = band_limit(p.nx, p.lx, p.dealias), My = band_limit(p.ny, p.ly, p.dealias),
+              Mz = band_limit(p.nz, p.lz, p.dealias);
+    const double pkx = (double)((Mx + 1 + 3) / 4 * 4), nkyc = 2.0 * My + 1, nkzc = 2.0 * Mz + 1;
+    const double csize = nkzc * nkyc * pkx, zsize = (double)p.nz * nkyc * pkx, ysize = (double)p.nz * p.ny * pkx;
+    const double ncell = (double)p.nx * p.ny * p.nz;
+    const int nm = p.nz > 1 ? 3 : (p.ny > 1 ? 2 : 1);
+    const bool grad = std::string(p.terms).find("gradient") != std::string::npos;
+    const bool evolve = std::string(p.closure) == "maxwell";
+    const int ninA = 1 + nm + (grad ? nm + 1 : 0), noutA = nm + nm * (nm + 1) / 2 + 1;
+    const int ninB = nm + (evolve ? 6 * nm : 0), noutB = nm + (evolve ? 6 : 0);
+    const int nin = std::max({ninA, ninB, 10}), nout = std::max({noutA, noutB, 10});
+    double bytes = cb * (68.0 * csize + nin * zsize + (p.ny > 1 ? nin * ysize : 0.0) + nout * ysize) +
+                   b * (14.0 * ncell + csize);
+    if (std::string(p.kind) == "electron") bytes += 8.0 * 6 * 6601;
+    bytes += 64.0 * 1024;   // twiddles, control block, reduction partials
+    return bytes;
+}
+
 int build_setup(const hydft_params *pin, const hydft_structure *st_in, int device, ModelHost &mh, std::string &err)
 {
     hydft_params p = *pin;

@@ -40,5 +40,8 @@ void params_default(hydft_params *p);
 void params_finalize(hydft_params *p);
 int params_read(const char *path, hydft_params *p, std::string &err);
 int build_setup(const hydft_params *p, const hydft_structure *st, int device, ModelHost &mh, std::string &err);
+// device bytes a model of these parameters allocates (the solver's buffers,
+// assuming Pi evolves whenever the closure is Maxwell); -1 if invalid
+double footprint_bytes(const hydft_params *p);
 
 }  // namespace hydft

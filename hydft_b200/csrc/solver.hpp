@@ -68,6 +68,13 @@ public:
     virtual void enqueue_steps(int k) = 0;
     // records that steps enqueued earlier (a replayed ensemble graph) ran
     virtual void mark_advanced() = 0;
+    // k replays of the captured step graph on this solver's stream, without
+    // waiting for them or reading the status word (poll_status does that)
+    virtual int launch_steps(int k) = 0;
+    // waits for this solver's stream and turns its status word into a code
+    virtual int poll_status() = 0;
+    // bytes of device memory this solver allocated
+    virtual size_t device_bytes() const = 0;
     // device address of the status word the step kernels set (ST_* bits)
     virtual const unsigned *status_word() const = 0;
     // turns status bits read from status_word() into an error code and

@@ -231,6 +231,7 @@ public:
     bool host_pending = false;   // a Maxwell relaxation waits for u of the new state
     bool fast_x = false;         // x passes on the register FFT (3-D grids, planned nx)
     bool staged_x = true;        // xa_regs / xb_rows (HYDFT_XPASS=v1 selects xa_fast / xb_fast)
+    size_t alloc_bytes = 0;      // device memory allocated by this solver
     int num_sms = 148;
 
     // per-kernel CUDA-event timing (profile mode, uncaptured steps only)
@@ -306,6 +307,7 @@ public:
             return HYDFT_E_OOM;
         }
         allocs.push_back(q);
+        alloc_bytes += std::max<size_t>(n, 1) * sizeof(T);
         p = static_cast<T *>(q);
         return 0;
     }
@@ -985,6 +987,16 @@ public:
 
     int advance(int nsteps) override
     {
+        if (int rc = launch_steps(nsteps)) return rc;
+        return check_status();
+    }
+
+    int poll_status() override { return check_status(); }
+
+    size_t device_bytes() const override { return alloc_bytes; }
+
+    int launch_steps(int nsteps) override
+    {
         if (nsteps <= 0) return 0;
         if (!gexec) {
             const int64_t before = launches;
@@ -1003,7 +1015,7 @@ public:
         }
         host_pending = ph.evolve != 0;
         CK(cudaGetLastError());
-        return check_status();
+        return 0;
     }
 
     int rhs(double t, double *dn, double *dmom, double *dpi) override

@@ -116,6 +116,13 @@ def lib():
         L.hydft_gpu_fourier_bessel.argtypes = [_P, _P, _I, _D, _I, _I]
         L.hydft_gpu_fd_table.argtypes = [_I, _P, C.POINTER(_I)]
         L.hydft_gpu_fd_alpha.argtypes = [_I, _P, _P, _I]
+        L.hydft_gpu_footprint.argtypes = [C.POINTER(Params), C.POINTER(_D)]
+        L.hydft_serve_create.argtypes = [_I, _D, _I, _I, C.POINTER(_P)]
+        L.hydft_serve_submit.argtypes = [_P, C.POINTER(Params), _P, _P, _P, _I, _I, C.POINTER(C.c_int64)]
+        L.hydft_serve_wait.argtypes = [_P, C.c_int64, _D, C.POINTER(_I)]
+        L.hydft_serve_result.argtypes = [_P, C.c_int64, _P, _P, _P, _P]
+        L.hydft_serve_stats.argtypes = [_P, _P]
+        L.hydft_serve_destroy.argtypes = [_P]
         L.hydft_batch_create.argtypes = [_I, _P, _P, _I, C.POINTER(_P)]
         L.hydft_batch_destroy.argtypes = [_P]
         L.hydft_batch_size.argtypes = [_P]
@@ -455,6 +462,90 @@ class Batch:
                 m.h = None
             lib().hydft_batch_destroy(self.b)
             self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def footprint(p):
+    """Device bytes a model of params p allocates (hydft_gpu_footprint)."""
+    b = _D()
+    rc = lib().hydft_gpu_footprint(C.byref(p), C.byref(b))
+    if rc:
+        raise HydftError(rc, "invalid grid")
+    return b.value
+
+
+REQ_QUEUED, REQ_SETUP, REQ_RUNNING, REQ_DONE, REQ_FAILED = range(5)
+INFO_KEYS = ("t", "dt", "step", "mass", "mom_x", "mom_y", "mom_z", "ekin", "nmin", "nmax",
+             "t_submit", "t_admit", "t_start", "t_done", "bytes", "launches")
+
+
+class Server:
+    """Continuous-batching solve server on one GPU (hydft_serve_*)."""
+
+    def __init__(self, device=0, hbm_budget=0.0, max_slots=64, chunk_steps=50):
+        b = _P()
+        rc = lib().hydft_serve_create(device, float(hbm_budget), max_slots, chunk_steps, C.byref(b))
+        if rc:
+            raise HydftError(rc, lib().hydft_gpu_create_error().decode())
+        self.s = b
+        self._shapes = {}
+
+    def submit(self, p, nsteps, state=None, keep_state=False):
+        """Queue a solve of params p for nsteps steps; state = (n, mom, pi)
+        host arrays or None for p's initial condition.  Returns its id."""
+        rid = C.c_int64()
+        keep = []
+        ptrs = [None, None, None]
+        if state is not None:
+            shp = (p.nz, p.ny, p.nx)
+            n = np.ascontiguousarray(state[0], dtype=np.float64).reshape(shp)
+            mom = np.zeros((3,) + shp) if state[1] is None else np.ascontiguousarray(state[1], dtype=np.float64)
+            pi = None if len(state) < 3 or state[2] is None else np.ascontiguousarray(state[2], dtype=np.float64)
+            keep = [n, mom, pi]
+            ptrs = [_ptr(n), _ptr(mom), _ptr(pi)]
+        rc = lib().hydft_serve_submit(self.s, C.byref(p), ptrs[0], ptrs[1], ptrs[2], int(nsteps),
+                                      1 if keep_state else 0, C.byref(rid))
+        if rc:
+            raise HydftError(rc, lib().hydft_gpu_create_error().decode())
+        self._shapes[rid.value] = ((p.nz, p.ny, p.nx), p.closure.decode() == "maxwell", keep_state)
+        return rid.value
+
+    def wait(self, rid, timeout=-1.0):
+        st = _I()
+        rc = lib().hydft_serve_wait(self.s, rid, float(timeout), C.byref(st))
+        if rc:
+            raise HydftError(rc, "unknown request %d" % rid)
+        return st.value
+
+    def result(self, rid):
+        """Final scalars (dict) and, if kept, fields (n, mom, pi) of a finished
+        request; raises HydftError if it failed.  Releases the request."""
+        shp, maxwell, keep = self._shapes.pop(rid)
+        info = np.zeros(16)
+        n = mom = pi = None
+        if keep:
+            n = np.zeros(shp)
+            mom = np.zeros((3,) + shp)
+            pi = np.zeros((6,) + shp) if maxwell else None
+        rc = lib().hydft_serve_result(self.s, rid, _ptr(n), _ptr(mom), _ptr(pi), _ptr(info))
+        if rc:
+            raise HydftError(rc, lib().hydft_gpu_create_error().decode())
+        return dict(zip(INFO_KEYS, info.tolist())), (n, mom, pi)
+
+    def stats(self):
+        v = np.zeros(6)
+        lib().hydft_serve_stats(self.s, _ptr(v))
+        return dict(zip(("queued", "holding", "completed", "max_holding", "bytes_in_use", "budget"), v.tolist()))
+
+    def close(self):
+        if getattr(self, "s", None):
+            lib().hydft_serve_destroy(self.s)
+            self.s = None
 
     def __del__(self):
         try:

@@ -281,6 +281,51 @@ int hydft_batch_failed_member(const hydft_batch *b);
 int64_t hydft_batch_launch_count(const hydft_batch *b);
 void *hydft_batch_stream(const hydft_batch *b);
 
+/* Device bytes a model of these parameters allocates (the admission size
+ * the server uses; Pi is assumed to evolve whenever the closure is Maxwell). */
+int hydft_gpu_footprint(const hydft_params *p, double *bytes);
+
+/*
+ * Serving: solve requests on one GPU with continuous batching.  No
+ * counterpart in the reference (each request runs the driver loop of
+ * src/hydft.f90:41-51 for its model).
+ *
+ * hydft_serve_create starts a server on `device` with an HBM budget in
+ * bytes (0: 80 % of the free memory), at most max_slots requests holding
+ * device memory at once, and chunk_steps RK3 steps launched per scheduling
+ * round of a request.  hydft_serve_submit queues a request: a model of *p,
+ * its initial state (n, mom, pi host arrays as for hydft_gpu_set_state, or
+ * n == NULL for p's initial condition), nsteps steps at p->dt (or the CFL
+ * dt of hydft_gpu_compute_dt when p->dt is 0), keep_state != 0 to keep the
+ * final fields.  Requests are admitted in arrival order as their footprint
+ * (hydft_gpu_footprint) fits the budget; the models of admitted requests
+ * stay resident and their steps overlap on the device.  A request larger
+ * than the whole budget is refused (HYDFT_ERR_OOM).
+ * hydft_serve_wait blocks until request `id` is done or failed (timeout_s <
+ * 0: no limit) and reports its HYDFT_REQ_* state.  hydft_serve_result
+ * copies the final fields (when kept) and HYDFT_SERVE_INFO_LEN scalars into
+ * info: t, dt, step, mass, mom[3], ekin, nmin, nmax, then the submit,
+ * admit, first-launch and completion times in seconds since the server
+ * started, the footprint in bytes and the kernels launched; it returns the
+ * request's status and releases it (message: hydft_gpu_create_error()).
+ * hydft_serve_stats fills 6 values: queued, holding memory, completed,
+ * most held at once, bytes in use, budget.
+ */
+#define HYDFT_REQ_QUEUED 0
+#define HYDFT_REQ_SETUP 1
+#define HYDFT_REQ_RUNNING 2
+#define HYDFT_REQ_DONE 3
+#define HYDFT_REQ_FAILED 4
+#define HYDFT_SERVE_INFO_LEN 16
+typedef struct hydft_server hydft_server;
+int hydft_serve_create(int device, double hbm_budget_bytes, int max_slots, int chunk_steps, hydft_server **out);
+int hydft_serve_submit(hydft_server *s, const hydft_params *p, const double *n, const double *mom,
+                       const double *pi, int nsteps, int keep_state, int64_t *id);
+int hydft_serve_wait(hydft_server *s, int64_t id, double timeout_s, int *state);
+int hydft_serve_result(hydft_server *s, int64_t id, double *n, double *mom, double *pi, double *info);
+int hydft_serve_stats(hydft_server *s, double *stats);
+void hydft_serve_destroy(hydft_server *s);
+
 #ifdef __cplusplus
 }
 #endif

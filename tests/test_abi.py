@@ -83,3 +83,14 @@ def test_create_fails_loudly_without_gpu():
     with pytest.raises(hg.HydftError) as e:
         hg.Model(hg.default_params(nx=16))
     assert e.value.code == 7
+
+
+def test_footprint_of_the_256_maxwell_step():
+    import hydft_b200 as hg
+    kw = dict(kind="ion", nx=256, ny=256, nz=256, lx=64.0, ly=64.0, lz=64.0, closure="maxwell")
+    f32 = hg.footprint(hg.default_params(gpu_precision="fp32", **kw))
+    f64 = hg.footprint(hg.default_params(gpu_precision="fp64", **kw))
+    newt = hg.footprint(hg.default_params(gpu_precision="fp32", **dict(kw, closure="newtonian")))
+    assert 3.5e9 < f32 < 5.0e9
+    assert abs(f64 / f32 - 2.0) < 0.01
+    assert newt < f32
