@@ -282,7 +282,10 @@ int hydft_gpu_budgets(hydft_gpu *h, double *mass, double mom[3], double *ekin, d
     if (mom)
         for (int d = 0; d < 3; ++d) mom[d] = sm[d] / nc * v;
     if (ekin) *ekin = 0.5 * (sk / nc) * v / h->mh.mass;
-    if (fe) *fe = NAN;   // free energy of the functional: not computed on the device yet
+    if (fe) {
+        rc = h->s->energy(fe);
+        if (rc) return wrap(h, rc);
+    }
     if (nmin) *nmin = mn;
     if (nmax) *nmax = mx;
     return HYDFT_OK;

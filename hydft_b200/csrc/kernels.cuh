@@ -278,6 +278,10 @@ struct Ctrl {
     double pend_phi, pend_e; // relaxation factors of the pending stage
     unsigned status;
     int pending;             // Maxwell relaxation pending
+    // external potential as last evaluated (vext_t%v after the last rhs):
+    // amplitude and exp(-i omega t) of that time
+    double v_amp, v_ewr, v_ewi;
+    double gf[3];            // mean of n F_ext for the gaussian potential, stage start
 };
 
 // physics constants for the pointwise and spectral kernels
@@ -372,6 +376,7 @@ struct PWB {
     const R *dn_real, *u_real;
     size_t ncell;
     const cplx<double> *ex, *ey, *ez;   // exp(i k_d x_d) per axis
+    const R *gradv;                      // grad of the gaussian potential (3 fields)
     const Ctrl *ctrl;
     int stage;
     unsigned *status;
@@ -382,7 +387,9 @@ struct PWB {
         const double nref = (double)nhat[0].x;
         const R n = R(nref + (double)dn_real[q]);
         R f[3] = {R(0), R(0), R(0)};
-        if (ph.ext_active) {
+        if (ph.ext_active && ph.ext_kind == 3) {
+            for (int d = 0; d < nm; ++d) f[d] = -gradv[d * ncell + q];
+        } else if (ph.ext_active) {
             const int y = row % g.ny, z = row / g.ny;
             const StageScal &s = ctrl->st[stage];
             cplx<double> e = ex[x] * ey[y];
@@ -596,6 +603,8 @@ __global__ void combine_b_kernel(Grid g, Phys ph, int nm, CombineB<R> c, Ctrl *c
                 if (ph.ext_active && ph.ext_kind != 3) {
                     const double im = s.ewi * ctrl->nkd_re - s.ewr * ctrl->nkd_im;
                     mf = s.amp * ph.ext_k[i] * im;
+                } else if (ph.ext_active) {
+                    mf = ctrl->gf[i];
                 }
                 dm[i] = cplx<R>{R(mf), R(0)};
             }
@@ -712,6 +721,42 @@ static __global__ void end_step_kernel(Ctrl *ctrl)
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     ctrl->t = ctrl->t + ctrl->dt;
     ctrl->step = ctrl->step + 1;
+    // the last right-hand side of the step was evaluated at stage 3's time
+    ctrl->v_amp = ctrl->st[2].amp;
+    ctrl->v_ewr = ctrl->st[2].ewr;
+    ctrl->v_ewi = ctrl->st[2].ewi;
+}
+
+// one probe record: t, n and mom_x at compact index idx (conjugated when
+// the mode is stored as its mirror), into ring slot *count
+template <typename R>
+__global__ void probe_kernel(const Ctrl *ctrl, const cplx<R> *N, const cplx<R> *M0, long long idx, int conj,
+                             double *ring, int *count, int cap)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int slot = *count;
+    if (slot >= cap) return;
+    double nr = 0.0, ni = 0.0, mr = 0.0, mi = 0.0;
+    if (idx >= 0) {
+        nr = (double)N[idx].x;
+        ni = (double)N[idx].y;
+        mr = (double)M0[idx].x;
+        mi = (double)M0[idx].y;
+        if (conj) { ni = -ni; mi = -mi; }
+    }
+    double *r = ring + 5 * (size_t)slot;
+    r[0] = ctrl->t;
+    r[1] = nr; r[2] = ni; r[3] = mr; r[4] = mi;
+    *count = slot + 1;
+}
+
+// the potential of a right-hand side evaluated at stage `stage`'s time
+static __global__ void vlast_kernel(Ctrl *ctrl, int stage)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    ctrl->v_amp = ctrl->st[stage].amp;
+    ctrl->v_ewr = ctrl->st[stage].ewr;
+    ctrl->v_ewi = ctrl->st[stage].ewi;
 }
 
 }  // namespace hydft

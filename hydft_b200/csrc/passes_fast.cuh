@@ -412,7 +412,10 @@ __global__ void __launch_bounds__(256, HYDFT_XMINB) xb_fast(Grid g, XFastArgs<R>
             const int xx = block_pos<T, E>(t, r);
             const R n = rowok ? nref + pw.dn_real[rowbase + xx] : R(0);
             R f0 = R(0), f1 = R(0);
-            if (pw.ph.ext_active) {
+            if (pw.ph.ext_active && pw.ph.ext_kind == 3) {
+                f0 = rowok ? -pw.gradv[(size_t)i0 * pw.ncell + rowbase + xx] : R(0);
+                if (i1 < NM) f1 = rowok ? -pw.gradv[(size_t)i1 * pw.ncell + rowbase + xx] : R(0);
+            } else if (pw.ph.ext_active) {
                 const StageScal &s = pw.ctrl->st[pw.stage];
                 cplx<double> e = pw.ex[xx] * pw.ey[y];
                 e = e * pw.ez[z];
@@ -590,8 +593,10 @@ __host__ __device__ constexpr int xreal_stride() { return T * E + T; }
 // Phase B with this block's real-space rows (dn and, when Pi evolves, u_d)
 // copied into shared memory by cp.async at the start; the copies overlap the
 // first inverse transform, and the spectral inputs are prefetched to L2 a few
-// fields ahead.  Same inputs, outputs and arithmetic as xb_fast.
-template <typename R, int T, int E, bool EVOLVE, bool EXT>
+// fields ahead.  Same inputs, outputs and arithmetic as xb_fast.  EXTK: no
+// external force (0), a plane-wave potential (1), the gaussian potential's
+// static force field (2).
+template <typename R, int T, int E, bool EVOLVE, int EXTK>
 __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xb_rows(Grid g, XFastArgs<R> a, const cplx<R> *twx, PWB<R> pw)
 {
     constexpr int L = T * E, NM = 3;
@@ -644,7 +649,11 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xb_rows(Grid g, XFa
             const int xx = block_pos<T, E>(t, r);
             const R n = nref + nrow[xx];
             R f0 = R(0), f1 = R(0);
-            if (EXT) {
+            if (EXTK == 2) {
+                const size_t q = (size_t)row * L + xx;
+                f0 = rowok ? -pw.gradv[(size_t)i0 * pw.ncell + q] : R(0);
+                if (i1 < NM) f1 = rowok ? -pw.gradv[(size_t)i1 * pw.ncell + q] : R(0);
+            } else if (EXTK == 1) {
                 const StageScal &s = pw.ctrl->st[pw.stage];
                 cplx<double> e = pw.ex[xx] * pw.ey[y];
                 e = e * pw.ez[z];

@@ -385,8 +385,12 @@ double footprint_bytes(const hydft_params *pin)
     const int nin = std::max({ninA, ninB, 10}), nout = std::max({noutA, noutB, 10});
     double bytes = cb * (68.0 * csize + nin * zsize + (p.ny > 1 ? nin * ysize : 0.0) + nout * ysize) +
                    b * (14.0 * ncell + csize);
+    const std::string terms = p.terms;
+    if (terms.find("hartree") != std::string::npos) bytes += b * csize;   // v(k) for the energy
+    if (terms.find("ry") != std::string::npos) bytes += b * csize;        // c_cor(k) for the energy
+    if (std::string(p.vext) == "gaussian") bytes += b * 4.0 * ncell + cb * csize;
     if (std::string(p.kind) == "electron") bytes += 8.0 * 6 * 6601;
-    bytes += 64.0 * 1024;   // twiddles, control block, reduction partials
+    bytes += 96.0 * 1024;   // twiddles, control block, reduction partials
     return bytes;
 }
 
@@ -671,6 +675,42 @@ int build_setup(const hydft_params *pin, const hydft_structure *st_in, int devic
                 S.klin[((size_t)kzc * g.nkyc + kyc) * g.pkx + kxc] = v;
             }
 
+    // free-energy terms in input order and the hartree / RY kernels apart
+    S.neterms = 0;
+    for (auto &t : terms) {
+        int id = 0;
+        if (t == "ideal") id = 1;
+        else if (t == "tf") id = 2;
+        else if (t == "gradient") id = 3;
+        else if (t == "hartree") id = 4;
+        else if (t == "ry") id = 5;
+        if (id && S.neterms < 8) S.eterm_order[S.neterms++] = id;
+    }
+    {
+        bool hh = false, rr = false;
+        for (auto &t : terms) {
+            hh = hh || t == "hartree";
+            rr = rr || t == "ry";
+        }
+        if (hh) S.kh.assign(csize, 0.0);
+        if (rr) S.kr.assign(csize, 0.0);
+        S.vk0 = hh ? mh.hartree_kernel(0.0) : 0.0;
+        S.ck0 = rr ? mh.c_cor(0.0) : 0.0;
+        if (hh || rr)
+            for (int kzc = 0; kzc < g.nkzc; ++kzc)
+                for (int kyc = 0; kyc < g.nkyc; ++kyc)
+                    for (int kxc = 0; kxc < g.nkxc; ++kxc) {
+                        const int my = signed_idx(kyc, g.My), mz = signed_idx(kzc, g.Mz);
+                        const double kx = TWOPI * kxc / p.lx;
+                        const double ky = p.ny > 1 ? TWOPI * my / p.ly : 0.0;
+                        const double kz = p.nz > 1 ? TWOPI * mz / p.lz : 0.0;
+                        const double kabs = std::sqrt(kx * kx + ky * ky + kz * kz);
+                        const size_t q = ((size_t)kzc * g.nkyc + kyc) * g.pkx + kxc;
+                        if (hh) S.kh[q] = mh.hartree_kernel(kabs);
+                        if (rr) S.kr[q] = mh.c_cor(kabs);
+                    }
+    }
+
     // external potential (external_potential.f90:39-63)
     const std::string vx = p.vext;
     S.ext_active = 0;
@@ -683,7 +723,21 @@ int build_setup(const hydft_params *pin, const hydft_structure *st_in, int devic
         err = "unknown external potential: " + vx;
         return HYDFT_ERR_UNSUPPORTED;
     }
-    if (S.ext_kind == 3) { err = "external potential 'gaussian' is not implemented on the GPU path"; return HYDFT_ERR_UNSUPPORTED; }
+    if (S.ext_kind == 3) {
+        // v = -A exp(-r^2 / (2 w^2)) about the box centre (external_potential.f90:81-91)
+        const size_t nc = (size_t)p.nx * p.ny * p.nz;
+        S.gauss_v.assign(nc, 0.0);
+        const double w2 = p.vext_width * p.vext_width;
+        for (int k = 0; k < p.nz; ++k)
+            for (int j = 0; j < p.ny; ++j)
+                for (int i = 0; i < p.nx; ++i) {
+                    const double x = i * (p.lx / p.nx) - 0.5 * p.lx;
+                    const double y = p.ny > 1 ? j * (p.ly / p.ny) - 0.5 * p.ly : 0.0;
+                    const double z = p.nz > 1 ? k * (p.lz / p.nz) - 0.5 * p.lz : 0.0;
+                    const double r2 = x * x + y * y + z * z;
+                    S.gauss_v[i + (size_t)p.nx * (j + (size_t)p.ny * k)] = -p.vext_amplitude * std::exp(-0.5 * r2 / w2);
+                }
+    }
     S.ext_k[0] = TWOPI * p.vext_mode[0] / p.lx;
     S.ext_k[1] = p.ny > 1 ? TWOPI * p.vext_mode[1] / p.ly : 0.0;
     S.ext_k[2] = p.nz > 1 ? TWOPI * p.vext_mode[2] / p.lz : 0.0;

@@ -30,7 +30,14 @@ struct SolverSetup {
     std::vector<double> klin;         // compact band, sum of hartree/ry mu kernels
     std::vector<double> fdtab;        // 6*6601, electrons only
     std::vector<std::complex<double>> ex, ey, ez;
-    std::vector<double> gauss_f;      // gaussian external force (3 real fields), optional
+    std::vector<double> gauss_v;      // gaussian external potential on the grid (ext_kind 3)
+    // free energy (functional_t%energy): term ids in input order (1 ideal,
+    // 2 tf, 3 gradient, 4 hartree, 5 ry), hartree v(k) and RY c_cor(k) on
+    // the compact band, and both at k = 0
+    int eterm_order[8] = {0};
+    int neterms = 0;
+    std::vector<double> kh, kr;
+    double vk0 = 0, ck0 = 0;
 };
 
 struct KernelStat {
@@ -51,6 +58,9 @@ public:
     virtual int reductions(double *sum_n, double sum_m[3], double *sum_m2n, double *nmin,
                            double *nmax, double *umax) = 0;
     virtual int mode(int field, int mx, int my, int mz, double *re, double *im) = 0;
+    // functional_t%energy plus the external-potential energy of the current
+    // state (diagnostics.f90:41-60), FP64
+    virtual int energy(double *fe) = 0;
     virtual void set_time(double t, double dt) = 0;
     virtual void get_time(double *t, double *dt, int64_t *step) = 0;
     virtual void *stream() = 0;
@@ -75,6 +85,17 @@ public:
     virtual int poll_status() = 0;
     // bytes of device memory this solver allocated
     virtual size_t device_bytes() const = 0;
+    virtual void set_step(int64_t step) = 0;
+    // Probes (diag_t%probe, diagnostics.f90:70-77) recorded on the device:
+    // probe_setup picks the Fourier mode; launch_steps_probed runs k steps
+    // (graph replays) and after every step whose number is a multiple of
+    // `every` stores t and the n and mom_x coefficients of the mode (5
+    // doubles) in a device ring of probe_capacity() entries, read back and
+    // cleared by read_probes.
+    virtual int probe_setup(int mx, int my, int mz) = 0;
+    virtual int probe_capacity() const = 0;
+    virtual int launch_steps_probed(int k, int every) = 0;
+    virtual int read_probes(std::vector<double> &out) = 0;
     // device address of the status word the step kernels set (ST_* bits)
     virtual const unsigned *status_word() const = 0;
     // turns status bits read from status_word() into an error code and

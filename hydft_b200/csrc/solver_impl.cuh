@@ -138,6 +138,149 @@ __global__ void reduce_final_kernel(const RedPart *part, int nb, RedPart *out)
     *out = o;
 }
 
+
+// ------------------------------------------------ energies and force means
+// Up to 6 FP64 sums per block, each compensated (Neumaier) over the block's
+// grid-stride share, the lanes then combined in a fixed order: the result
+// does not depend on timing.
+constexpr int NSUM = 6;
+
+__device__ __forceinline__ void block_sums(double (&v)[NSUM], double *part)
+{
+    __shared__ double sh[NSUM][8];
+    for (int off = 16; off > 0; off >>= 1)
+        for (int i = 0; i < NSUM; ++i) v[i] += __shfl_down_sync(0xffffffffu, v[i], off);
+    const int w = threadIdx.x / 32, l = threadIdx.x % 32;
+    if (l == 0)
+        for (int i = 0; i < NSUM; ++i) sh[i][w] = v[i];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = blockDim.x / 32;
+        for (int i = 0; i < NSUM; ++i) {
+            double a = 0.0, c = 0.0;
+            for (int j = 0; j < nw; ++j) neumaier<double>(a, c, sh[i][j]);
+            part[blockIdx.x * NSUM + i] = a + c;
+        }
+    }
+}
+
+static __global__ void sums_final_kernel(const double *part, int nb, double *out)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    for (int i = 0; i < NSUM; ++i) {
+        double a = 0.0, c = 0.0;
+        for (int b = 0; b < nb; ++b) neumaier<double>(a, c, part[b * NSUM + i]);
+        out[i] = a + c;
+    }
+}
+
+// Hartree and RY energies by Parseval on the band, k != 0:
+// sums of w |n_k|^2 v(k) and w |n_k|^2 c_cor(k), w = 1 at kx = 0, else 2
+template <typename R>
+__global__ void energy_spec_kernel(Grid g, const cplx<R> *N, const R *Kh, const R *Kr, double *part)
+{
+    const size_t total = (size_t)g.nkzc * g.nkyc * g.pkx;
+    double a[2] = {0.0, 0.0}, c[2] = {0.0, 0.0};
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (size_t)gridDim.x * blockDim.x) {
+        int kxc, kyc, kzc;
+        kvec(g, idx, kxc, kyc, kzc);
+        if (kxc >= g.nkxc || (kxc == 0 && kyc == 0 && kzc == 0)) continue;
+        const double w = kxc == 0 ? 1.0 : 2.0;
+        const double re = (double)N[idx].x, im = (double)N[idx].y;
+        const double a2 = w * (re * re + im * im);
+        if (Kh) neumaier<double>(a[0], c[0], a2 * (double)Kh[idx]);
+        if (Kr) neumaier<double>(a[1], c[1], a2 * (double)Kr[idx]);
+    }
+    double v[NSUM] = {a[0] + c[0], a[1] + c[1], 0.0, 0.0, 0.0, 0.0};
+    block_sums(v, part);
+}
+
+// Real-space sums over the grid: 2 ideal n(ln n - 1), 3 TF n alpha -
+// (2/3) c_n I_{3/2}(alpha), 4 gradient xi(alpha) |grad n|^2, 5 external n v
+struct EnergyReal {
+    double nref;
+    const double *fdtab;
+    double cn;
+    int ideal, tf, grad, ext;      // ext: 0 none, 1 plane wave, 2 gaussian
+    const cplx<double> *ex, *ey, *ez;
+    const Ctrl *ctrl;
+};
+
+template <typename R>
+__global__ void energy_real_kernel(Grid g, const R *dn, const R *gn, const R *gv, size_t ncell, EnergyReal e,
+                                   double *part)
+{
+    double a[4] = {0.0, 0.0, 0.0, 0.0}, c[4] = {0.0, 0.0, 0.0, 0.0};
+    double vamp = 0.0, vr = 1.0, vi = 0.0;
+    if (e.ext == 1) {
+        vamp = e.ctrl->v_amp;
+        vr = e.ctrl->v_ewr;
+        vi = e.ctrl->v_ewi;
+    }
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < ncell; q += (size_t)gridDim.x * blockDim.x) {
+        const double n = e.nref + (double)dn[q];
+        if (e.ideal) neumaier<double>(a[0], c[0], n * (log(n) - 1.0));
+        if (e.tf || e.grad) {
+            bool ok = true;
+            const double al = fd::alpha_from_ip12(e.fdtab, n / e.cn, &ok);
+            if (e.tf) neumaier<double>(a[1], c[1], n * al - (2.0 / 3.0) * e.cn * fd::ip32(e.fdtab, al));
+            if (e.grad) {
+                double g2 = 0.0;
+                for (int d = 0; d < 3; ++d) {
+                    const double gd = (double)gn[d * ncell + q];
+                    g2 += gd * gd;
+                }
+                neumaier<double>(a[2], c[2], fd::xi(e.fdtab, al) * g2);
+            }
+        }
+        if (e.ext == 1) {
+            const int x = (int)(q % g.nx), y = (int)((q / g.nx) % g.ny), z = (int)(q / ((size_t)g.nx * g.ny));
+            cplx<double> ph = e.ex[x] * e.ey[y];
+            ph = ph * e.ez[z];
+            const double v = vamp * (ph.x * vr - ph.y * vi);
+            neumaier<double>(a[3], c[3], n * v);
+        } else if (e.ext == 2) {
+            neumaier<double>(a[3], c[3], n * (double)gv[q]);
+        }
+    }
+    double v[NSUM] = {0.0, 0.0, a[0] + c[0], a[1] + c[1], a[2] + c[2], a[3] + c[3]};
+    block_sums(v, part);
+}
+
+// mean of n F for the gaussian potential, F = -grad v:
+// sum over the band of w k_i Im(conj(n_k) v_k)
+template <typename R>
+__global__ void gauss_force_mean_kernel(Grid g, const cplx<R> *N, const cplx<R> *V, double *part)
+{
+    const size_t total = (size_t)g.nkzc * g.nkyc * g.pkx;
+    double a[3] = {0.0, 0.0, 0.0}, c[3] = {0.0, 0.0, 0.0};
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (size_t)gridDim.x * blockDim.x) {
+        int kxc, kyc, kzc;
+        kvec(g, idx, kxc, kyc, kzc);
+        if (kxc >= g.nkxc) continue;
+        const double w = kxc == 0 ? 1.0 : 2.0;
+        const double nr = (double)N[idx].x, ni = (double)N[idx].y;
+        const double vr = (double)V[idx].x, vi = (double)V[idx].y;
+        const double im = nr * vi - ni * vr;   // Im(conj(n) v)
+        const double k[3] = {kxc * g.kx0, signed_idx(kyc, g.My) * g.ky0, signed_idx(kzc, g.Mz) * g.kz0};
+        for (int d = 0; d < 3; ++d) neumaier<double>(a[d], c[d], w * k[d] * im);
+    }
+    double v[NSUM] = {a[0] + c[0], a[1] + c[1], a[2] + c[2], 0.0, 0.0, 0.0};
+    block_sums(v, part);
+}
+
+static __global__ void gauss_force_final_kernel(const double *part, int nb, Ctrl *ctrl)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    for (int i = 0; i < 3; ++i) {
+        double a = 0.0, c = 0.0;
+        for (int b = 0; b < nb; ++b) neumaier<double>(a, c, part[b * NSUM + i]);
+        ctrl->gf[i] = a + c;
+    }
+}
+
 template <typename R>
 __global__ void fill_real_kernel(R *dst, const double *src, double sub, size_t n)
 {
@@ -221,6 +364,15 @@ public:
     cplx<double> *ex, *ey, *ez;
     cplx<R> *twx, *twy, *twz;
     cplx<R> *tpx = nullptr, *tpy = nullptr, *tpz = nullptr;   // planned tables of the register passes
+    R *Kh = nullptr, *Kr = nullptr;        // hartree v(k), RY c_cor(k) on the band (energy)
+    R *gV = nullptr, *gG = nullptr;        // gaussian potential and its gradient (3 fields), real space
+    cplx<R> *Vg = nullptr;                 // gaussian potential on the band
+    double *spart = nullptr, *sout = nullptr;   // block partials and results of the 6-sum reductions
+    double *pring = nullptr;                    // probe records (5 doubles each)
+    int *pcount = nullptr;
+    long long pidx = -1;
+    int pconj = 0;
+    static constexpr int PROBE_CAP = 4096;
     Ctrl *ctrl;
     RedPart *rpart, *rout;
     int red_blocks = 0;
@@ -442,11 +594,27 @@ public:
         {
             Ctrl c;
             std::memset(&c, 0, sizeof(c));
+            // vext_t%setup evaluates the potential at t = 0 (external_potential.f90:56)
+            c.v_amp = (s.ext_td && s.ext_ramp > 0.0) ? 0.0 : s.ext_amp;
+            c.v_ewr = 1.0;
+            c.v_ewi = 0.0;
             CK(cudaMemcpy(ctrl, &c, sizeof(c), cudaMemcpyHostToDevice));
         }
         red_blocks = 2 * 148;
         if (int rc = alloc(rpart, red_blocks)) return rc;
         if (int rc = alloc(rout, 1)) return rc;
+        if (int rc = alloc(spart, (size_t)red_blocks * NSUM)) return rc;
+        if (int rc = alloc(sout, NSUM)) return rc;
+        auto up_band = [&](R *&dst, const std::vector<double> &v) -> int {
+            if (v.empty()) return 0;
+            if (int rc = alloc(dst, csize)) return rc;
+            std::vector<R> h(csize, R(0));
+            for (size_t i = 0; i < csize && i < v.size(); ++i) h[i] = R(v[i]);
+            CK(cudaMemcpy(dst, h.data(), csize * sizeof(R), cudaMemcpyHostToDevice));
+            return 0;
+        };
+        if (int rc = up_band(Kh, s.kh)) return rc;
+        if (int rc = up_band(Kr, s.kr)) return rc;
         // x-pass rows per block
         xrb_a = pick_rb(ninA, noutA);
         xrb_b = pick_rb(ninB, noutB);
@@ -473,6 +641,26 @@ public:
             const char *ev = std::getenv("HYDFT_XPASS");
             if (ev && std::string(ev) == "v1") staged_x = false;
             CK(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
+        }
+        if (s.ext_active && s.ext_kind == 3) {
+            // the gaussian potential, its band spectrum and its spectral gradient
+            // (vext_eval: F = -grad v, external_potential.f90:81-91)
+            if (int rc = alloc(gV, ncell)) return rc;
+            if (int rc = alloc(gG, 3 * ncell)) return rc;
+            if (int rc = alloc(Vg, csize)) return rc;
+            if (int rc = up(gV, s.gauss_v.data(), 1, 0.0)) return rc;
+            const R *src1[1] = {gV};
+            cplx<R> *dst1[1] = {Vg};
+            if (int rc = from_real(1, src1, dst1)) return rc;
+            const cplx<R> *src3[3] = {Vg, Vg, Vg};
+            int ops3[3] = {OP_IKX, OP_IKY, OP_IKZ};
+            CK(cudaMemsetAsync(gG, 0, 3 * ncell * sizeof(R), st));
+            inverse(nm, src3, ops3);
+            PWToReal<R> pw;
+            for (int f = 0; f < MAXF; ++f) pw.dst[f] = f < nm ? gG + (size_t)f * ncell : nullptr;
+            pw.ncell = ncell;
+            x_toreal(nm, pw);
+            CK(cudaGetLastError());
         }
         // uniform initial state n = n0, mom = 0, Pi = 0 (species.f90:155-169)
         set_k0_kernel<R><<<1, 32, 0, st>>>(N, s.n0);
@@ -710,13 +898,15 @@ public:
                 const int rb = nt / T;
                 launch("xpass_b", xbytes(nin, nout, nreal), [&] { k<<<(nrows + rb - 1) / rb, nt, sm, st>>>(g, a, tpx, pw); });
             };
-            const bool ext = ph.ext_active != 0;
+            const int extk = !ph.ext_active ? 0 : (ph.ext_kind == 3 ? 2 : 1);
             if (staged_x && ph.evolve) {
-                if (ext) go_rows(xb_rows<R, T, E, true, true>, 4);
-                else go_rows(xb_rows<R, T, E, true, false>, 4);
+                if (extk == 2) go_rows(xb_rows<R, T, E, true, 2>, 4);
+                else if (extk == 1) go_rows(xb_rows<R, T, E, true, 1>, 4);
+                else go_rows(xb_rows<R, T, E, true, 0>, 4);
             } else if (staged_x) {
-                if (ext) go_rows(xb_rows<R, T, E, false, true>, 1);
-                else go_rows(xb_rows<R, T, E, false, false>, 1);
+                if (extk == 2) go_rows(xb_rows<R, T, E, false, 2>, 1);
+                else if (extk == 1) go_rows(xb_rows<R, T, E, false, 1>, 1);
+                else go_rows(xb_rows<R, T, E, false, 0>, 1);
             } else if (ph.evolve) {
                 go(xb_fast<R, T, E, 3, true>);
             } else {
@@ -823,10 +1013,18 @@ public:
         pw.u_real = u_real;
         pw.ncell = ncell;
         pw.ex = ex; pw.ey = ey; pw.ez = ez;
+        pw.gradv = gG;
         pw.ctrl = ctrl;
         pw.stage = stage;
         pw.status = &ctrl->status;
         const int nout = nm + (ph.evolve ? 6 : 0);
+        if (ph.ext_active && ph.ext_kind == 3) {
+            // mean of n F over the stage state (k = 0 of the momentum tendency)
+            launch("force_mean", 0.0, [&] {
+                gauss_force_mean_kernel<R><<<red_blocks, 256, 0, st>>>(g, N, Vg, spart);
+            });
+            launch("force_mean", 0.0, [&] { gauss_force_final_kernel<<<1, 32, 0, st>>>(spart, red_blocks, ctrl); });
+        }
         if (fast_x) xb_launch(nf, nout, pw, ph.evolve ? 1 + nm : 1);
         else xpass(nf, nout, pw, xrb_b, "xpass_b", ph.evolve ? 1 + nm : 1);
         forward(nout, OB);
@@ -993,6 +1191,72 @@ public:
 
     int poll_status() override { return check_status(); }
 
+    void set_step(int64_t step) override
+    {
+        Ctrl c;
+        cudaMemcpyAsync(&c, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st);
+        cudaStreamSynchronize(st);
+        c.step = step;
+        cudaMemcpyAsync(ctrl, &c, sizeof(Ctrl), cudaMemcpyHostToDevice, st);
+        cudaStreamSynchronize(st);
+    }
+
+    int probe_capacity() const override { return PROBE_CAP; }
+
+    int probe_setup(int mx, int my, int mz) override
+    {
+        if (!pring) {
+            if (int rc = alloc(pring, (size_t)5 * PROBE_CAP)) return rc;
+            if (int rc = alloc(pcount, 1)) return rc;
+        }
+        CK(cudaMemsetAsync(pcount, 0, sizeof(int), st));
+        // the compact index of the mode, as in mode()
+        pconj = 0;
+        if (mx < 0) { mx = -mx; my = -my; mz = -mz; pconj = 1; }
+        auto wrapm = [](int m, int n) { m = ((m % n) + n) % n; return m <= n / 2 ? m : m - n; };
+        my = g.ny > 1 ? wrapm(my, g.ny) : 0;
+        mz = g.nz > 1 ? wrapm(mz, g.nz) : 0;
+        if (mx > g.Mx || std::abs(my) > g.My || std::abs(mz) > g.Mz) {
+            pidx = -1;
+        } else {
+            const int kyc = my >= 0 ? my : my + 2 * g.My + 1;
+            const int kzc = mz >= 0 ? mz : mz + 2 * g.Mz + 1;
+            pidx = ((long long)kzc * g.nkyc + kyc) * g.pkx + mx;
+        }
+        return 0;
+    }
+
+    int launch_steps_probed(int k, int every) override
+    {
+        if (!pring) { err = "probe_setup was not called"; return HYDFT_E_BAD; }
+        Ctrl c;
+        CK(cudaMemcpyAsync(&c, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        long long step = c.step;
+        for (int i = 0; i < k; ++i) {
+            if (int rc = launch_steps(1)) return rc;
+            ++step;
+            if (every > 0 && step % every == 0) {
+                probe_kernel<R><<<1, 32, 0, st>>>(ctrl, N, M[0], pidx, pconj, pring, pcount, PROBE_CAP);
+                launches++;
+            }
+        }
+        CK(cudaGetLastError());
+        return 0;
+    }
+
+    int read_probes(std::vector<double> &out) override
+    {
+        int cnt = 0;
+        CK(cudaMemcpyAsync(&cnt, pcount, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        out.assign((size_t)5 * cnt, 0.0);
+        if (cnt) CK(cudaMemcpyAsync(out.data(), pring, sizeof(double) * 5 * cnt, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemsetAsync(pcount, 0, sizeof(int), st));
+        CK(cudaStreamSynchronize(st));
+        return 0;
+    }
+
     size_t device_bytes() const override { return alloc_bytes; }
 
     int launch_steps(int nsteps) override
@@ -1030,6 +1294,8 @@ public:
         begin_step();
         phase_a(0, ph.evolve != 0);
         phase_b(0, true);
+        vlast_kernel<<<1, 32, 0, st>>>(ctrl, 0);
+        launches++;
         set_time(t0, dt0);
         CK(cudaGetLastError());
         if (int rc = check_status()) return rc;
@@ -1217,6 +1483,66 @@ public:
         *nmin = h.nmin;
         *nmax = h.nmax;
         *umax = h.umax;
+        return 0;
+    }
+
+    int energy(double *fe) override
+    {
+        const int ngr = ph.has_grad ? nm : 0;
+        const cplx<R> *src[4] = {N, N, N, N};
+        int ops[4] = {OP_ZK0, OP_IKX, OP_IKY, OP_IKZ};
+        inverse(1 + ngr, src, ops);
+        PWToReal<R> pw;
+        for (int f = 0; f < MAXF; ++f) pw.dst[f] = nullptr;
+        pw.dst[0] = io_real;
+        for (int d = 0; d < ngr; ++d) pw.dst[1 + d] = io_real + (size_t)(1 + d) * ncell;
+        pw.ncell = ncell;
+        if (ph.has_grad && nm < 3)
+            CK(cudaMemsetAsync(io_real + (size_t)(1 + nm) * ncell, 0, (3 - nm) * ncell * sizeof(R), st));
+        x_toreal(1 + ngr, pw);
+        cplx<R> h0;
+        CK(cudaMemcpyAsync(&h0, N, sizeof(h0), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        const double nmean = (double)h0.x;
+        double spec[NSUM], real[NSUM];
+        energy_spec_kernel<R><<<red_blocks, 256, 0, st>>>(g, N, Kh, Kr, spart);
+        sums_final_kernel<<<1, 32, 0, st>>>(spart, red_blocks, sout);
+        CK(cudaMemcpyAsync(spec, sout, sizeof(spec), cudaMemcpyDeviceToHost, st));
+        EnergyReal e;
+        e.nref = nmean;
+        e.fdtab = fdtab;
+        e.cn = S.cn;
+        e.ideal = ph.has_ideal;
+        e.tf = ph.has_tf;
+        e.grad = ph.has_grad;
+        e.ext = !ph.ext_active ? 0 : (ph.ext_kind == 3 ? 2 : 1);
+        e.ex = ex; e.ey = ey; e.ez = ez;
+        e.ctrl = ctrl;
+        energy_real_kernel<R><<<red_blocks, 256, 0, st>>>(g, io_real, io_real + ncell, gV, ncell, e, spart);
+        sums_final_kernel<<<1, 32, 0, st>>>(spart, red_blocks, sout);
+        CK(cudaMemcpyAsync(real, sout, sizeof(real), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        launches += 4;
+        CK(cudaGetLastError());
+        // terms in input order (functional.f90:80-90), each mean * volume
+        const double nc = (double)ncell, vol = S.volume, beta = S.beta;
+        double f = 0.0;
+        for (int i = 0; i < S.neterms; ++i) {
+            switch (S.eterm_order[i]) {
+            case 1: f += real[2] / nc * vol / beta; break;
+            case 2: f += real[3] / nc * vol / beta; break;
+            case 3: f += S.cg * real[4] / nc * vol; break;
+            case 4: f += 0.5 * (spec[0] + S.vk0 * nmean * nmean) * vol; break;
+            case 5: {
+                const double b0 = nmean - S.n0;
+                f += -0.5 * (spec[1] + S.ck0 * b0 * b0) * vol / beta;
+                break;
+            }
+            default: break;
+            }
+        }
+        if (ph.ext_active) f += real[5] / nc * vol;
+        *fe = f;
         return 0;
     }
 

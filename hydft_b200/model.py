@@ -117,6 +117,9 @@ def lib():
         L.hydft_gpu_fd_table.argtypes = [_I, _P, C.POINTER(_I)]
         L.hydft_gpu_fd_alpha.argtypes = [_I, _P, _P, _I]
         L.hydft_gpu_footprint.argtypes = [C.POINTER(Params), C.POINTER(_D)]
+        L.hydft_gpu_write_fields.argtypes = [_P, C.c_char_p]
+        L.hydft_gpu_read_fields.argtypes = [_P, C.c_char_p]
+        L.hydft_gpu_run.argtypes = [_P]
         L.hydft_serve_create.argtypes = [_I, _D, _I, _I, C.POINTER(_P)]
         L.hydft_serve_submit.argtypes = [_P, C.POINTER(Params), _P, _P, _P, _I, _I, C.POINTER(C.c_int64)]
         L.hydft_serve_wait.argtypes = [_P, C.c_int64, _D, C.POINTER(_I)]
@@ -261,6 +264,20 @@ class Model:
         md = (_I * 3)(*mode)
         self._check(lib().hydft_gpu_set_initial_condition(self.h, kind.encode(), amplitude, md,
                                                           width, seed))
+
+    # -- files and the driver loop
+    def write_fields(self, prefix):
+        """write_fields: <prefix>_fld_NNNNNN.bin in the reference's format."""
+        self._check(lib().hydft_gpu_write_fields(self.h, str(prefix).encode()))
+
+    def read_fields(self, path):
+        """Resume from a .bin field file (state, t; step from the name)."""
+        self._check(lib().hydft_gpu_read_fields(self.h, str(path).encode()))
+
+    def run(self):
+        """hydft_run's loop from the current state, writing the prefix's
+        _diag.dat, _probe.dat (and _fld_*.bin when iout > 0)."""
+        self._check(lib().hydft_gpu_run(self.h))
 
     # -- stepping
     def advance(self, nsteps=1):

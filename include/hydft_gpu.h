@@ -281,6 +281,20 @@ int hydft_batch_failed_member(const hydft_batch *b);
 int64_t hydft_batch_launch_count(const hydft_batch *b);
 void *hydft_batch_stream(const hydft_batch *b);
 
+/* write_fields (src/model/io.f90:19-35): <prefix>_fld_NNNNNN.bin (NNNNNN =
+ * step), raw little-endian: int32 nx, ny, nz, ndim, npi; float64 t, lx,
+ * ly, lz; then n, mom(3), Pi(npi) in Fortran order. */
+int hydft_gpu_write_fields(hydft_gpu *h, const char *prefix);
+/* Resume from a field file of that format (no counterpart in the
+ * reference, whose python/hydft_io.py:45-56 only reads them): the state and
+ * t are set from the file, the step from its name; dt is kept. */
+int hydft_gpu_read_fields(hydft_gpu *h, const char *path);
+/* hydft_run's loop (src/hydft.f90:30-60) from the current state: dt from
+ * compute_dt every 20 steps, the last step ending at tend, probes every
+ * iprobe steps into <prefix>_probe.dat, budgets every idiag steps into
+ * <prefix>_diag.dat, fields every iout steps (diagnostics.f90:32-77). */
+int hydft_gpu_run(hydft_gpu *h);
+
 /* Device bytes a model of these parameters allocates (the admission size
  * the server uses; Pi is assumed to evolve whenever the closure is Maxwell). */
 int hydft_gpu_footprint(const hydft_params *p, double *bytes);

@@ -129,6 +129,17 @@ CASES = {
                                        closure="newtonian"),
     "fast_ion_maxwell_16x16x256": dict(ION, nx=16, ny=16, nz=256, lx=8.0, ly=8.0, lz=64.0,
                                        closure="maxwell", tau_model="constant", tau=0.7),
+    # the gaussian external potential (static force from its spectral gradient)
+    "ion_gaussian_3d": dict(ION, nx=16, ny=12, nz=8, lx=20.0, ly=15.0, lz=10.0, closure="newtonian",
+                            vext="gaussian", vext_amplitude=0.05, vext_width=2.5),
+    "fast_ion_gaussian_32x32x32": dict(ION, nx=32, ny=32, nz=32, lx=16.0, ly=16.0, lz=16.0,
+                                       closure="newtonian", vext="gaussian", vext_amplitude=0.05,
+                                       vext_width=2.0),
+    "fast_ion_maxwell_gaussian_32x48x32": dict(ION, nx=32, ny=48, nz=32, lx=16.0, ly=24.0, lz=16.0,
+                                               closure="maxwell", tau_model="constant", tau=1.5,
+                                               vext="gaussian", vext_amplitude=0.05, vext_width=2.0),
+    "electron_gaussian_2d": dict(ELEC, nx=32, ny=16, nz=1, lx=20.0, ly=10.0, closure="newtonian",
+                                 vext="gaussian", vext_amplitude=0.02, vext_width=3.0),
 }
 
 
@@ -238,3 +249,26 @@ def test_nonpositive_density_is_an_error(hg):
     with pytest.raises(hg.HydftError) as e:
         m.advance(50)
     assert e.value.code in (3, 4)
+
+
+ENERGY_CASES = ["ion_newtonian_3d", "ion_maxwell_ichimaru", "electron_driven_3d", "ion_nodealias_mode",
+                "ion_gaussian_3d", "fast_ion_maxwell_gaussian_32x48x32", "electron_gaussian_2d", "ion_1d"]
+
+
+@pytest.mark.parametrize("case", ENERGY_CASES)
+def test_free_energy_matches_oracle(hg, orc, case):
+    """budgets' F (functional_t%energy + the external potential as last
+    evaluated, diagnostics.f90:41-60) against the oracle, before and after
+    steps."""
+    m, o = pair(hg, orc, dt=0.01, **CASES[case])
+    n, mom, pi = seeded_state(m)
+    m.set_state(n, mom, pi)
+    o.set_state(n, mom, pi)
+    fe = m.budgets()[3]
+    ofe = o.budgets()[3]
+    assert abs(fe - ofe) <= TOL64 * max(abs(ofe), 1e-300)
+    m.advance(3)
+    o.advance(3)
+    fe = m.budgets()[3]
+    ofe = o.budgets()[3]
+    assert abs(fe - ofe) <= TOL64 * max(abs(ofe), 1e-300)
