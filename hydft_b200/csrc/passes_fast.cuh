@@ -198,13 +198,10 @@ __host__ __device__ constexpr int xrow_stride() { return (T * E + E + 15) / 16 *
 // layout, then inverse FFT to block layout: v[r] = a(x) + i b(x) at
 // x = block_pos(t, r).  inb may be null (b = 0).
 template <typename R, int T, int E>
-__device__ __forceinline__ void x_c2r_pair(cplx<R> (&v)[E], const cplx<R> *__restrict__ ina,
-                                           const cplx<R> *__restrict__ inb, int row, bool rowok, int t,
-                                           const Grid &g, cplx<R> *xrow, const cplx<R> *tw)
+__device__ __forceinline__ void x_c2r_load(cplx<R> (&v)[E], const cplx<R> *__restrict__ ina,
+                                           const cplx<R> *__restrict__ inb, size_t base, bool rowok, int t, int Mx)
 {
     constexpr int L = T * E;
-    const int Mx = g.Mx;
-    const size_t base = (size_t)row * g.pkx;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
         const int k = t + T * e;
@@ -224,6 +221,14 @@ __device__ __forceinline__ void x_c2r_pair(cplx<R> (&v)[E], const cplx<R> *__res
         }
         v[e] = Z;
     }
+}
+
+template <typename R, int T, int E>
+__device__ __forceinline__ void x_c2r_pair(cplx<R> (&v)[E], const cplx<R> *__restrict__ ina,
+                                           const cplx<R> *__restrict__ inb, int row, bool rowok, int t,
+                                           const Grid &g, cplx<R> *xrow, const cplx<R> *tw)
+{
+    x_c2r_load<R, T, E>(v, ina, inb, (size_t)row * g.pkx, rowok, t, g.Mx);
     stride_to_block<T, E, +1, R, BarWarp, 1>(v, t, xrow, tw);
 }
 
@@ -460,6 +465,21 @@ __device__ __forceinline__ void cp_async16(void *dst_smem, const void *src_gmem)
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src_gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// wait until at most one committed group of this thread is still in flight
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// cp.async of `rows` consecutive x rows of a spectral field (row stride pkx,
+// rows contiguous) starting at row0 into dst[rows][pkx]; every thread of the
+// block takes a share of the 16-byte chunks
+template <typename R>
+__device__ __forceinline__ void stage_rows(cplx<R> *dst, const cplx<R> *src, int row0, int rows, int pkx, int tid,
+                                           int nt)
+{
+    const int chunks = (int)((size_t)rows * pkx * sizeof(cplx<R>) / 16);
+    const char *s = reinterpret_cast<const char *>(src + (size_t)row0 * pkx);
+    char *d = reinterpret_cast<char *>(dst);
+    for (int i = tid; i < chunks; i += nt) cp_async16(d + 16 * (size_t)i, s + 16 * (size_t)i);
+}
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // bulk prefetch of a 16-byte aligned global range (a multiple of 16 bytes)
@@ -601,14 +621,16 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xb_rows(Grid g, XFa
 {
     constexpr int L = T * E, NM = 3;
     constexpr int RS = xreal_stride<T, E>();
-    constexpr int CPR = L * (int)sizeof(R) / 16;   // 16-byte chunks per row
+    constexpr int CPR = L * (int)sizeof(R) / 16;   // 16-byte chunks per real row
     constexpr int EPC = 16 / (int)sizeof(R);        // elements per chunk
-    constexpr int AHEAD = 6;                        // fields prefetched ahead
+    constexpr int AHEAD = 6;                        // fields prefetched to L2 ahead
+    constexpr int NPAIR = EVOLVE ? 2 + 3 * NM : 2;  // (dmu_0, dmu_1), (dmu_2), (dPi pairs)
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
-    cplx<R> *xbuf = tw + 2 * L;
-    const int nt = blockDim.x, rb = nt / T;
-    R *rs = reinterpret_cast<R *>(xbuf + rb * xrow_stride<T, E>());   // [field][rb][RS]
+    const int nt = blockDim.x, rb = nt / T, pk = g.pkx;
+    cplx<R> *sb = tw + 2 * L;                       // [2][rb][pkx] the staged input pair
+    cplx<R> *xbuf = sb + 2 * (size_t)rb * pk;
+    R *rs = reinterpret_cast<R *>(xbuf + rb * xrow_stride<T, E>());   // [3][rb][RS] u rows
     const int tid = threadIdx.x, t = tid % T, rr = tid / T;
     const int nrows = g.ny * g.nz;
     const int row0 = blockIdx.x * rb;
@@ -616,43 +638,66 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xb_rows(Grid g, XFa
     const bool rowok = row < nrows;
     cplx<R> *xrow = xbuf + rr * xrow_stride<T, E>();
     const int vrows = max(0, min(rb, nrows - row0));
-    {
-        const int nf = EVOLVE ? 1 + NM : 1;
-        const int total = nf * vrows * CPR;
+    const size_t rowbase = (size_t)row * L;
+    // fields of pair p: (0, 1), (2, -), then (3 + 2q, 4 + 2q)
+    auto fields = [&](int p, int &fa, int &fb) {
+        if (p == 0) { fa = 0; fb = 1; }
+        else if (p == 1) { fa = 2; fb = -1; }
+        else { fa = NM + 2 * (p - 2); fb = fa + 1; }
+    };
+    auto stage = [&](int p) {
+        if (p >= NPAIR) return;
+        int fa, fb;
+        fields(p, fa, fb);
+        stage_rows(sb, a.in[fa], row0, vrows, pk, tid, nt);
+        if (fb >= 0) stage_rows(sb + (size_t)rb * pk, a.in[fb], row0, vrows, pk, tid, nt);
+        cp_async_commit();
+    };
+    // pair 0 and the u rows on their way; dn from global into registers
+    stage(0);
+    if (EVOLVE) {
+        const int total = NM * vrows * CPR;
         for (int i = tid; i < total; i += nt) {
             const int c = i % CPR, j = (i / CPR) % vrows, f = i / (CPR * vrows);
-            const R *src = (f == 0 ? pw.dn_real : pw.u_real + (size_t)(f - 1) * pw.ncell) + (size_t)(row0 + j) * L + c * EPC;
+            const R *src = pw.u_real + (size_t)f * pw.ncell + (size_t)(row0 + j) * L + c * EPC;
             cp_async16(rs + ((size_t)f * rb + j) * RS + c * EPC, src);
         }
         cp_async_commit();
     }
     XPrefetch<R> pf(a, g, row0, vrows, tid == 0);
     pf.upto(AHEAD);
+    R dnv[E];
+#pragma unroll
+    for (int r = 0; r < E; ++r) dnv[r] = rowok ? pw.dn_real[rowbase + block_pos<T, E>(t, r)] : R(0);
     for (int i = tid; i < 2 * L; i += nt) tw[i] = twx[i];
-    __syncthreads();
+    // the staged pair p into registers, then pair p + 1 on its way
+    auto load = [&](int p, cplx<R> (&v)[E]) {
+        int fa, fb;
+        fields(p, fa, fb);
+        cp_async_wait_all();
+        __syncthreads();
+        x_c2r_load<R, T, E>(v, sb, fb >= 0 ? sb + (size_t)rb * pk : nullptr, (size_t)rr * pk, rowok, t, g.Mx);
+        __syncthreads();
+        stage(p + 1);
+        pf.upto((fb >= 0 ? fb : fa) + 2 + AHEAD);
+    };
     const R nref = pw.nhat[0].x;
     const int y = rowok ? row % g.ny : 0, z = rowok ? row / g.ny : 0;
-    const R *nrow = rs + rr * RS;
     // n (dmu - F): pairs of components
 #pragma unroll
     for (int q = 0; 2 * q < NM; ++q) {
         const int i0 = 2 * q, i1 = 2 * q + 1;
         cplx<R> v[E];
-        pf.upto(i1 + AHEAD);
-        x_c2r_pair<R, T, E>(v, a.in[i0], i1 < NM ? a.in[i1] : nullptr, row, rowok, t, g, xrow, tw);
-        if (q == 0) {
-            cp_async_wait_all();
-            __syncthreads();
-        }
+        load(q, v);
+        stride_to_block<T, E, +1, R, BarWarp, 1>(v, t, xrow, tw);
 #pragma unroll
         for (int r = 0; r < E; ++r) {
             const int xx = block_pos<T, E>(t, r);
-            const R n = nref + nrow[xx];
+            const R n = nref + dnv[r];
             R f0 = R(0), f1 = R(0);
             if (EXTK == 2) {
-                const size_t q = (size_t)row * L + xx;
-                f0 = rowok ? -pw.gradv[(size_t)i0 * pw.ncell + q] : R(0);
-                if (i1 < NM) f1 = rowok ? -pw.gradv[(size_t)i1 * pw.ncell + q] : R(0);
+                f0 = rowok ? -pw.gradv[(size_t)i0 * pw.ncell + rowbase + xx] : R(0);
+                if (i1 < NM) f1 = rowok ? -pw.gradv[(size_t)i1 * pw.ncell + rowbase + xx] : R(0);
             } else if (EXTK == 1) {
                 const StageScal &s = pw.ctrl->st[pw.stage];
                 cplx<double> e = pw.ex[xx] * pw.ey[y];
@@ -675,11 +720,10 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xb_rows(Grid g, XFa
             for (int r = 0; r < E; ++r) acc[r] = cplx<R>{R(0), R(0)};
 #pragma unroll
             for (int d = 0; d < NM; ++d) {
-                const int f = NM + 2 * (cp * NM + d);
                 cplx<R> v[E];
-                pf.upto(f + 1 + AHEAD);
-                x_c2r_pair<R, T, E>(v, a.in[f], a.in[f + 1], row, rowok, t, g, xrow, tw);
-                const R *urow = rs + ((1 + d) * rb + rr) * RS;
+                load(2 + cp * NM + d, v);
+                stride_to_block<T, E, +1, R, BarWarp, 1>(v, t, xrow, tw);
+                const R *urow = rs + ((size_t)d * rb + rr) * RS;
 #pragma unroll
                 for (int r = 0; r < E; ++r) acc[r] = acc[r] - urow[block_pos<T, E>(t, r)] * v[r];
             }
@@ -688,14 +732,16 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xb_rows(Grid g, XFa
     }
 }
 
-// shared-memory bytes of a staged x pass
+// shared-memory bytes of the staged x passes: twiddles, staged spectral
+// rows (nstage fields), exchange rows, staged real rows (nreal fields)
 template <typename R, int T, int E>
-inline size_t xstaged_smem(int nt, int nreal)
+inline size_t xstaged_smem(int nt, int pkx, int nstage, int nreal)
 {
     const int rb = nt / T;
-    return sizeof(cplx<R>) * (2 * (size_t)T * E + (size_t)rb * xrow_stride<T, E>()) +
+    return sizeof(cplx<R>) * (2 * (size_t)T * E + (size_t)nstage * rb * pkx + (size_t)rb * xrow_stride<T, E>()) +
            sizeof(R) * (size_t)nreal * rb * xreal_stride<T, E>();
 }
+
 
 // Real-space I/O: half spectra -> real fields (TOREAL) or back.
 template <typename R, int T, int E, bool TOREAL>

@@ -854,7 +854,7 @@ public:
             };
             auto go_regs = [&](auto k) {
                 const int nt = 256 / T * T;
-                const size_t sm = xstaged_smem<R, T, E>(nt, 0);
+                const size_t sm = xstaged_smem<R, T, E>(nt, g.pkx, 0, 0);
                 set_smem(k, sm);
                 const int rb = nt / T;
                 launch(name, xbytes(nin, nout, nreal), [&] { k<<<(nrows + rb - 1) / rb, nt, sm, st>>>(g, a, tpx, pw); });
@@ -889,10 +889,11 @@ public:
             };
             auto go_rows = [&](auto k, int nreal_rows) {
                 int nt = 256 / T * T;
-                size_t sm = xstaged_smem<R, T, E>(nt, nreal_rows);
-                while (sm > 110 * 1024 && nt > T) {
+                size_t sm = xstaged_smem<R, T, E>(nt, g.pkx, 2, nreal_rows);
+                // two blocks per SM: 228 KB of shared memory, 1 KB reserved per block
+                while (sm > 115712 && nt > T) {
                     nt /= 2;
-                    sm = xstaged_smem<R, T, E>(nt, nreal_rows);
+                    sm = xstaged_smem<R, T, E>(nt, g.pkx, 2, nreal_rows);
                 }
                 set_smem(k, sm);
                 const int rb = nt / T;
@@ -900,13 +901,13 @@ public:
             };
             const int extk = !ph.ext_active ? 0 : (ph.ext_kind == 3 ? 2 : 1);
             if (staged_x && ph.evolve) {
-                if (extk == 2) go_rows(xb_rows<R, T, E, true, 2>, 4);
-                else if (extk == 1) go_rows(xb_rows<R, T, E, true, 1>, 4);
-                else go_rows(xb_rows<R, T, E, true, 0>, 4);
+                if (extk == 2) go_rows(xb_rows<R, T, E, true, 2>, 3);
+                else if (extk == 1) go_rows(xb_rows<R, T, E, true, 1>, 3);
+                else go_rows(xb_rows<R, T, E, true, 0>, 3);
             } else if (staged_x) {
-                if (extk == 2) go_rows(xb_rows<R, T, E, false, 2>, 1);
-                else if (extk == 1) go_rows(xb_rows<R, T, E, false, 1>, 1);
-                else go_rows(xb_rows<R, T, E, false, 0>, 1);
+                if (extk == 2) go_rows(xb_rows<R, T, E, false, 2>, 0);
+                else if (extk == 1) go_rows(xb_rows<R, T, E, false, 1>, 0);
+                else go_rows(xb_rows<R, T, E, false, 0>, 0);
             } else if (ph.evolve) {
                 go(xb_fast<R, T, E, 3, true>);
             } else {
