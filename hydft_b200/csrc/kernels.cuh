@@ -493,67 +493,100 @@ __global__ void combine_a_kernel(Grid g, Phys ph, int nm, CombineA<R> c, Ctrl *c
     const int pending = ctrl->pending;
     const double phi = ctrl->pend_phi;
     const double ee = ctrl->pend_e;
+    const int nf = nm * (nm + 1) / 2;
+    const bool need_u = ph.evolve || ph.newtonian;
+    const cplx<R> zero = {R(0), R(0)};
     for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
          idx += (size_t)gridDim.x * blockDim.x) {
         int kxc, kyc, kzc;
         kvec(g, idx, kxc, kyc, kzc);
         if (kxc >= g.nkxc) continue;
+        // every input of this element first (the stores below cannot move
+        // ahead of loads the compiler does not know are unaliased)
+        const cplx<R> nh = c.N[idx], gl = c.G[idx];
+        const R kl = c.Klin[idx];
+        cplx<R> F[6], U[3], Pv[6], P0v[6];
+#pragma unroll
+        for (int f = 0; f < 6; ++f) F[f] = f < nf ? c.F[f][idx] : zero;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) U[d] = (need_u && d < nm) ? c.U[d][idx] : zero;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            Pv[q] = ph.evolve ? c.P[q][idx] : zero;
+            P0v[q] = (ph.evolve && pending) ? c.P0[q][idx] : zero;
+        }
         const R k[3] = {R(kxc * g.kx0), R(signed_idx(kyc, g.My) * g.ky0), R(signed_idx(kzc, g.Mz) * g.kz0)};
         const bool k0 = kxc == 0 && kyc == 0 && kzc == 0;
         // chemical potential: local part + spectral kernels
-        cplx<R> mu = c.G[idx] + c.Klin[idx] * c.N[idx];
-        if (k0) mu = cplx<R>{R(0), R(0)};
-        c.MU[idx] = mu;
+        cplx<R> mu = gl + kl * nh;
+        if (k0) mu = zero;
         // divergence of the momentum flux
         cplx<R> D[3];
-        for (int i = 0; i < nm; ++i) {
-            cplx<R> s = {R(0), R(0)};
-            for (int j = 0; j < nm; ++j) s = s + ik_times(k[j], c.F[sym_idx(i, j, nm)][idx]);
-            D[i] = s;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            cplx<R> sm = zero;
+            if (i < nm)
+                for (int j = 0; j < nm; ++j) sm = sm + ik_times(k[j], F[sym_idx(i, j, nm)]);
+            D[i] = sm;
         }
-        cplx<R> fpi[3] = {{R(0), R(0)}, {R(0), R(0)}, {R(0), R(0)}};
+        cplx<R> fpi[3] = {zero, zero, zero};
+        cplx<R> p0[6], pc[6];
         if (ph.evolve) {
             // Pi0 of the stage-start velocity, completes the previous stage's relaxation
-            cplx<R> ku = {R(0), R(0)};
-            for (int d = 0; d < nm; ++d) ku = ku + ik_times(k[d], c.U[d][idx]);   // i k.u
+            cplx<R> ku = zero;
+            for (int d = 0; d < nm; ++d) ku = ku + ik_times(k[d], U[d]);   // i k.u
             const R eta = R(ph.eta), xi = R(ph.xi);
-            cplx<R> p0[6];
+#pragma unroll
             for (int ii = 0; ii < 3; ++ii) {
-                const cplx<R> du = ii < nm ? ik_times(k[ii], c.U[ii][idx]) : cplx<R>{R(0), R(0)};
+                const cplx<R> du = ii < nm ? ik_times(k[ii], U[ii]) : zero;
                 p0[ii] = eta * (R(2) * du - R(2.0 / 3.0) * ku) + xi * ku;
             }
             const int pi_i[3] = {0, 0, 1}, pi_j[3] = {1, 2, 2};
+#pragma unroll
             for (int q = 0; q < 3; ++q) {
                 const int i = pi_i[q], j = pi_j[q];
-                cplx<R> a1 = i < nm ? ik_times(k[j], c.U[i][idx]) : cplx<R>{R(0), R(0)};
-                cplx<R> a2 = j < nm ? ik_times(k[i], c.U[j][idx]) : cplx<R>{R(0), R(0)};
+                cplx<R> a1 = i < nm ? ik_times(k[j], U[i]) : zero;
+                cplx<R> a2 = j < nm ? ik_times(k[i], U[j]) : zero;
                 p0[3 + q] = eta * (a1 + a2);
             }
-            cplx<R> pc[6];
+#pragma unroll
             for (int q = 0; q < 6; ++q) {
-                cplx<R> p = c.P[q][idx];
+                cplx<R> pv = Pv[q];
                 if (pending) {
-                    const cplx<R> po = c.P0[q][idx];
-                    p = p0[q] - R(phi) * (p0[q] - po) + R(ee) * (p - po);
-                    c.P[q][idx] = p;
+                    const cplx<R> po = P0v[q];
+                    pv = p0[q] - R(phi) * (p0[q] - po) + R(ee) * (pv - po);
                 }
-                pc[q] = p;
-                c.P0[q][idx] = p0[q];
+                pc[q] = pv;
             }
-            for (int i = 0; i < nm; ++i) {
-                cplx<R> s = {R(0), R(0)};
-                for (int j = 0; j < nm; ++j) s = s + ik_times(k[j], pc[pi_idx(i, j)]);
-                fpi[i] = s;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                cplx<R> sm = zero;
+                if (i < nm)
+                    for (int j = 0; j < nm; ++j) sm = sm + ik_times(k[j], pc[pi_idx(i, j)]);
+                fpi[i] = sm;
             }
         } else if (ph.newtonian) {
             // div Pi0 = eta lap u + (eta/3 + xi) grad div u, spectrally
-            cplx<R> kdu = {R(0), R(0)};
-            for (int d = 0; d < nm; ++d) kdu = kdu + k[d] * c.U[d][idx];
+            cplx<R> kdu = zero;
+            for (int d = 0; d < nm; ++d) kdu = kdu + k[d] * U[d];
             const R k2 = k[0] * k[0] + k[1] * k[1] + k[2] * k[2];
             const R eta = R(ph.eta), b = R(ph.eta / 3.0 + ph.xi);
-            for (int i = 0; i < nm; ++i) fpi[i] = R(-1) * (eta * k2 * c.U[i][idx] + (b * k[i]) * kdu);
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                if (i < nm) fpi[i] = R(-1) * (eta * k2 * U[i] + (b * k[i]) * kdu);
         }
-        for (int i = 0; i < nm; ++i) c.Q[i][idx] = fpi[i] - D[i];
+        // stores
+        c.MU[idx] = mu;
+        if (ph.evolve) {
+#pragma unroll
+            for (int q = 0; q < 6; ++q) {
+                if (pending) c.P[q][idx] = pc[q];
+                c.P0[q][idx] = p0[q];
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            if (i < nm) c.Q[i][idx] = fpi[i] - D[i];
         if (k0 && ph.ext_active) {
             // n hat at the drive mode, read before this stage's update
             if (ph.drive_in_band) {
@@ -583,22 +616,47 @@ __global__ void combine_b_kernel(Grid g, Phys ph, int nm, CombineB<R> c, Ctrl *c
     const StageScal s = ctrl->st[stage];
     const double dt = ctrl->dt;
     const R da = R(dt * s.a), db = R(dt * s.b);
+    const cplx<R> zero = {R(0), R(0)};
+    const bool regs = !rhs_only && stage != 0;   // the RK registers are read
     for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
          idx += (size_t)gridDim.x * blockDim.x) {
         int kxc, kyc, kzc;
         kvec(g, idx, kxc, kyc, kzc);
         if (kxc >= g.nkxc) continue;
+        // every input of this element first
+        cplx<R> M[3], Qv[3], Gv[3], RMv[3], Pv[6], Vv[6], RPv[6];
+        cplx<R> Nv = zero, RNv = zero;
+        if (!rhs_only) Nv = c.N[idx];
+        if (regs) RNv = c.RN[idx];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const bool on = d < nm;
+            M[d] = on ? c.M[d][idx] : zero;
+            Qv[d] = on ? c.Q[d][idx] : zero;
+            Gv[d] = on ? c.Gm[d][idx] : zero;
+            RMv[d] = (on && regs) ? c.RM[d][idx] : zero;
+        }
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            Vv[q] = ph.evolve ? c.V[q][idx] : zero;
+            Pv[q] = (ph.evolve && !rhs_only) ? c.P[q][idx] : zero;
+            RPv[q] = (ph.evolve && regs) ? c.RP[q][idx] : zero;
+        }
         const R k[3] = {R(kxc * g.kx0), R(signed_idx(kyc, g.My) * g.ky0), R(signed_idx(kzc, g.Mz) * g.kz0)};
         const bool k0 = kxc == 0 && kyc == 0 && kzc == 0;
-        cplx<R> dn = {R(0), R(0)};
-        for (int d = 0; d < nm; ++d) dn = dn + ik_times(k[d], c.M[d][idx]);
+        cplx<R> dn = zero;
+        for (int d = 0; d < nm; ++d) dn = dn + ik_times(k[d], M[d]);
         dn = R(-ph.inv_mass) * dn;
-        cplx<R> dm[3] = {{R(0), R(0)}, {R(0), R(0)}, {R(0), R(0)}};
-        for (int i = 0; i < nm; ++i) dm[i] = c.Q[i][idx] - c.Gm[i][idx];
+        cplx<R> dm[3] = {zero, zero, zero};
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            if (i < nm) dm[i] = Qv[i] - Gv[i];
         if (k0) {
             // mean of the internal force removed; mean of n F_ext kept:
             // <n A sin(k.r - w t)> = A Im(exp(-i w t) conj(nhat(k)))
-            for (int i = 0; i < nm; ++i) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                if (i >= nm) continue;
                 double mf = 0.0;
                 if (ph.ext_active && ph.ext_kind != 3) {
                     const double im = s.ewi * ctrl->nkd_re - s.ewr * ctrl->nkd_im;
@@ -611,25 +669,34 @@ __global__ void combine_b_kernel(Grid g, Phys ph, int nm, CombineB<R> c, Ctrl *c
         }
         if (rhs_only) {
             c.oN[idx] = dn;
+#pragma unroll
             for (int i = 0; i < 3; ++i) c.oM[i][idx] = dm[i];
             if (ph.evolve)
-                for (int q = 0; q < 6; ++q) c.oP[q][idx] = c.V[q][idx];
+#pragma unroll
+                for (int q = 0; q < 6; ++q) c.oP[q][idx] = Vv[q];
             continue;
         }
         if (stage == 0) {
-            c.N[idx] = c.N[idx] + da * dn;
-            for (int i = 0; i < nm; ++i) c.M[i][idx] = c.M[i][idx] + da * dm[i];
+            c.N[idx] = Nv + da * dn;
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                if (i < nm) c.M[i][idx] = M[i] + da * dm[i];
         } else {
-            c.N[idx] = c.N[idx] + (da * dn + db * c.RN[idx]);
-            for (int i = 0; i < nm; ++i) c.M[i][idx] = c.M[i][idx] + (da * dm[i] + db * c.RM[i][idx]);
+            c.N[idx] = Nv + (da * dn + db * RNv);
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                if (i < nm) c.M[i][idx] = M[i] + (da * dm[i] + db * RMv[i]);
         }
         c.RN[idx] = dn;
-        for (int i = 0; i < nm; ++i) c.RM[i][idx] = dm[i];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            if (i < nm) c.RM[i][idx] = dm[i];
         if (ph.evolve) {
+#pragma unroll
             for (int q = 0; q < 6; ++q) {
-                const cplx<R> v = c.V[q][idx];
-                if (stage == 0) c.P[q][idx] = c.P[q][idx] + da * v;
-                else c.P[q][idx] = c.P[q][idx] + (da * v + db * c.RP[q][idx]);
+                const cplx<R> v = Vv[q];
+                if (stage == 0) c.P[q][idx] = Pv[q] + da * v;
+                else c.P[q][idx] = Pv[q] + (da * v + db * RPv[q]);
                 c.RP[q][idx] = v;
             }
         }

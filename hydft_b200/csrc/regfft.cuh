@@ -15,26 +15,154 @@
 // same four-step rule inside the registers.
 #pragma once
 
+#include <type_traits>
+
 #include "common.cuh"
 #include "fft.cuh"
 
 namespace hydft {
 
-// W_N^j = exp(-2 pi i j/N) for the composite register DFTs, in constant
-// memory (indices are compile-time constants after unrolling).
-struct RegTw {
-    double w6[6][2], w12[12][2], w16[16][2], w24[24][2], w32[32][2];
-};
-static __constant__ RegTw c_regtw;
+// W_N^j = exp(-2 pi i j/N) = {cos, -sin}(2 pi j/N) for the composite
+// register DFTs, as compile-time constants: after unrolling every factor is
+// an immediate operand, and the quarter turns become sign changes and swaps.
+// f(integral_constant<int, i>) for i = 0 .. N-1, unrolled at compile time
+template <int I, int N, class F>
+__device__ __forceinline__ void unroll_for_impl(F &&f)
+{
+    if constexpr (I < N) {
+        f(std::integral_constant<int, I>{});
+        unroll_for_impl<I + 1, N>(f);
+    }
+}
+template <int N, class F>
+__device__ __forceinline__ void unroll_for(F &&f) { unroll_for_impl<0, N>(f); }
 
 template <int N>
-__device__ __forceinline__ const double *regtw_table()
+struct RegTwC;
+template <>
+struct RegTwC<6> {
+    static constexpr double w[6][2] = {{1.0, -0.0},
+                                      {0.5000000000000001, -0.8660254037844386},
+                                      {-0.4999999999999998, -0.8660254037844387},
+                                      {-1.0, -1.2246467991473532e-16},
+                                      {-0.5000000000000004, 0.8660254037844384},
+                                      {0.5000000000000001, 0.8660254037844386}};
+};
+template <>
+struct RegTwC<12> {
+    static constexpr double w[12][2] = {{1.0, -0.0},
+                                      {0.8660254037844387, -0.49999999999999994},
+                                      {0.5000000000000001, -0.8660254037844386},
+                                      {6.123233995736766e-17, -1.0},
+                                      {-0.4999999999999998, -0.8660254037844387},
+                                      {-0.8660254037844387, -0.49999999999999994},
+                                      {-1.0, -1.2246467991473532e-16},
+                                      {-0.8660254037844388, 0.4999999999999997},
+                                      {-0.5000000000000004, 0.8660254037844384},
+                                      {-1.8369701987210297e-16, 1.0},
+                                      {0.5000000000000001, 0.8660254037844386},
+                                      {0.8660254037844384, 0.5000000000000004}};
+};
+template <>
+struct RegTwC<16> {
+    static constexpr double w[16][2] = {{1.0, -0.0},
+                                      {0.9238795325112867, -0.3826834323650898},
+                                      {0.7071067811865476, -0.7071067811865475},
+                                      {0.38268343236508984, -0.9238795325112867},
+                                      {6.123233995736766e-17, -1.0},
+                                      {-0.3826834323650897, -0.9238795325112867},
+                                      {-0.7071067811865475, -0.7071067811865476},
+                                      {-0.9238795325112867, -0.3826834323650899},
+                                      {-1.0, -1.2246467991473532e-16},
+                                      {-0.9238795325112868, 0.38268343236508967},
+                                      {-0.7071067811865477, 0.7071067811865475},
+                                      {-0.38268343236509034, 0.9238795325112865},
+                                      {-1.8369701987210297e-16, 1.0},
+                                      {0.38268343236509, 0.9238795325112866},
+                                      {0.7071067811865474, 0.7071067811865477},
+                                      {0.9238795325112865, 0.3826834323650904}};
+};
+template <>
+struct RegTwC<24> {
+    static constexpr double w[24][2] = {{1.0, -0.0},
+                                      {0.9659258262890683, -0.25881904510252074},
+                                      {0.8660254037844387, -0.49999999999999994},
+                                      {0.7071067811865476, -0.7071067811865475},
+                                      {0.5000000000000001, -0.8660254037844386},
+                                      {0.25881904510252074, -0.9659258262890683},
+                                      {6.123233995736766e-17, -1.0},
+                                      {-0.25881904510252063, -0.9659258262890683},
+                                      {-0.4999999999999998, -0.8660254037844387},
+                                      {-0.7071067811865475, -0.7071067811865476},
+                                      {-0.8660254037844387, -0.49999999999999994},
+                                      {-0.9659258262890682, -0.258819045102521},
+                                      {-1.0, -1.2246467991473532e-16},
+                                      {-0.9659258262890683, 0.2588190451025208},
+                                      {-0.8660254037844388, 0.4999999999999997},
+                                      {-0.7071067811865479, 0.7071067811865471},
+                                      {-0.5000000000000004, 0.8660254037844384},
+                                      {-0.25881904510252063, 0.9659258262890683},
+                                      {-1.8369701987210297e-16, 1.0},
+                                      {0.2588190451025203, 0.9659258262890684},
+                                      {0.5000000000000001, 0.8660254037844386},
+                                      {0.7071067811865474, 0.7071067811865477},
+                                      {0.8660254037844384, 0.5000000000000004},
+                                      {0.9659258262890681, 0.25881904510252157}};
+};
+template <>
+struct RegTwC<32> {
+    static constexpr double w[32][2] = {{1.0, -0.0},
+                                      {0.9807852804032304, -0.19509032201612825},
+                                      {0.9238795325112867, -0.3826834323650898},
+                                      {0.8314696123025452, -0.5555702330196022},
+                                      {0.7071067811865476, -0.7071067811865475},
+                                      {0.5555702330196023, -0.8314696123025452},
+                                      {0.38268343236508984, -0.9238795325112867},
+                                      {0.19509032201612833, -0.9807852804032304},
+                                      {6.123233995736766e-17, -1.0},
+                                      {-0.1950903220161282, -0.9807852804032304},
+                                      {-0.3826834323650897, -0.9238795325112867},
+                                      {-0.555570233019602, -0.8314696123025455},
+                                      {-0.7071067811865475, -0.7071067811865476},
+                                      {-0.8314696123025453, -0.5555702330196022},
+                                      {-0.9238795325112867, -0.3826834323650899},
+                                      {-0.9807852804032304, -0.1950903220161286},
+                                      {-1.0, -1.2246467991473532e-16},
+                                      {-0.9807852804032304, 0.19509032201612836},
+                                      {-0.9238795325112868, 0.38268343236508967},
+                                      {-0.8314696123025455, 0.555570233019602},
+                                      {-0.7071067811865477, 0.7071067811865475},
+                                      {-0.5555702330196022, 0.8314696123025452},
+                                      {-0.38268343236509034, 0.9238795325112865},
+                                      {-0.19509032201612866, 0.9807852804032303},
+                                      {-1.8369701987210297e-16, 1.0},
+                                      {0.1950903220161283, 0.9807852804032304},
+                                      {0.38268343236509, 0.9238795325112866},
+                                      {0.5555702330196018, 0.8314696123025455},
+                                      {0.7071067811865474, 0.7071067811865477},
+                                      {0.8314696123025452, 0.5555702330196022},
+                                      {0.9238795325112865, 0.3826834323650904},
+                                      {0.9807852804032303, 0.19509032201612872}};
+};
+
+// x * exp(DIR i 2 pi j / N), j a compile-time constant
+template <int N, int J, int DIR, typename R>
+__device__ __forceinline__ cplx<R> twiddle_mul(cplx<R> x)
 {
-    if (N == 6) return &c_regtw.w6[0][0];
-    if (N == 12) return &c_regtw.w12[0][0];
-    if (N == 16) return &c_regtw.w16[0][0];
-    if (N == 24) return &c_regtw.w24[0][0];
-    return &c_regtw.w32[0][0];
+    constexpr int j = J % N;
+    if constexpr (j == 0) {
+        return x;
+    } else if constexpr (4 * j == N) {
+        return mul_i<DIR>(x);
+    } else if constexpr (2 * j == N) {
+        return cplx<R>{-x.x, -x.y};
+    } else if constexpr (4 * j == 3 * N) {
+        return mul_i<-DIR>(x);
+    } else {
+        constexpr double c = RegTwC<N>::w[j][0], sn = -RegTwC<N>::w[j][1];   // cos, sin
+        const R cr = R(c), si = R(DIR * sn);
+        return cplx<R>{x.x * cr - x.y * si, x.x * si + x.y * cr};
+    }
 }
 
 template <int N, int DIR, typename R>
@@ -67,21 +195,17 @@ struct RegDFTComp {
     static __device__ __forceinline__ void run(cplx<R> *v)
     {
         constexpr int N = A * B;
-        const double *w = regtw_table<N>();
         cplx<R> u[A][B];
-#pragma unroll
-        for (int a = 0; a < A; ++a) {
+        unroll_for<A>([&](auto ac) {
+            constexpr int a = decltype(ac)::value;
 #pragma unroll
             for (int b = 0; b < B; ++b) u[a][b] = v[a + A * b];
             RegDFT<B, DIR, R>::run(u[a]);
-#pragma unroll
-            for (int kb = 1; kb < B; ++kb) {
-                if (a == 0) continue;
-                const int j = (a * kb) % N;
-                const cplx<R> tw = {R(w[2 * j]), R(-DIR) * R(w[2 * j + 1])};
-                u[a][kb] = u[a][kb] * tw;
-            }
-        }
+            unroll_for<B>([&](auto kc) {
+                constexpr int kb = decltype(kc)::value;
+                u[a][kb] = twiddle_mul<N, a * kb, DIR>(u[a][kb]);
+            });
+        });
 #pragma unroll
         for (int kb = 0; kb < B; ++kb) {
             cplx<R> c[A];

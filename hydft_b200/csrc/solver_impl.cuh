@@ -620,22 +620,6 @@ public:
         xrb_b = pick_rb(ninB, noutB);
         xrb_io = pick_rb(10, 10);
         if (int rc = set_smem_attrs()) return rc;
-        {
-            RegTw rt;
-            const double pi = 3.14159265358979323846264338327950288;
-            auto fill = [&](double (*w)[2], int N) {
-                for (int j = 0; j < N; ++j) {
-                    w[j][0] = std::cos(2.0 * pi * j / N);
-                    w[j][1] = -std::sin(2.0 * pi * j / N);
-                }
-            };
-            fill(rt.w6, 6);
-            fill(rt.w12, 12);
-            fill(rt.w16, 16);
-            fill(rt.w24, 24);
-            fill(rt.w32, 32);
-            CK(cudaMemcpyToSymbol(c_regtw, &rt, sizeof(rt)));
-        }
         fast_x = has_plan(g.nx) && nm == 3;
         {
             const char *ev = std::getenv("HYDFT_XPASS");

@@ -115,6 +115,31 @@ module hydft_gpu_mod
       real(c_double), intent(out) :: t, dt
       integer(c_int64_t), intent(out) :: step
     end function
+    integer(c_int) function hydft_gpu_budgets(h, mass, mom, ekin, fe, nmin, nmax) bind(C, name='hydft_gpu_budgets')
+      import :: c_ptr, c_int, c_double
+      type(c_ptr), value :: h
+      real(c_double), intent(out) :: mass, mom(3), ekin, fe, nmin, nmax
+    end function
+    integer(c_int) function hydft_gpu_mode(h, field, mx, my, mz, re, im) bind(C, name='hydft_gpu_mode')
+      import :: c_ptr, c_int, c_double
+      type(c_ptr), value :: h
+      integer(c_int), value :: field, mx, my, mz
+      real(c_double), intent(out) :: re, im
+    end function
+    integer(c_int) function hydft_gpu_write_fields(h, prefix) bind(C, name='hydft_gpu_write_fields')
+      import :: c_ptr, c_int, c_char
+      type(c_ptr), value :: h
+      character(kind=c_char), intent(in) :: prefix(*)
+    end function
+    integer(c_int) function hydft_gpu_read_fields(h, path) bind(C, name='hydft_gpu_read_fields')
+      import :: c_ptr, c_int, c_char
+      type(c_ptr), value :: h
+      character(kind=c_char), intent(in) :: path(*)
+    end function
+    integer(c_int) function hydft_gpu_run(h) bind(C, name='hydft_gpu_run')
+      import :: c_ptr, c_int
+      type(c_ptr), value :: h
+    end function
   end interface
 
   !> model_t on the GPU: the state lives on the device and is copied to the
@@ -134,6 +159,10 @@ module hydft_gpu_mod
     procedure :: compute_dt => gpu_compute_dt
     procedure :: sync_to_host => gpu_sync_to_host
     procedure :: sync_to_device => gpu_sync_to_device
+    procedure :: budgets => gpu_budgets
+    procedure :: write_fields => gpu_write_fields
+    procedure :: read_fields => gpu_read_fields
+    procedure :: run => gpu_run
     procedure :: destroy => gpu_destroy
   end type model_gpu_t
 
@@ -177,6 +206,9 @@ contains
     call put(c%vext, p%vext)
     c%vext_amplitude = p%vext_amplitude; c%vext_mode = p%vext_mode
     c%vext_omega = p%vext_omega; c%vext_width = p%vext_width; c%vext_ramp = p%vext_ramp
+    c%nsteps_max = p%nsteps_max; c%iout = p%iout; c%iprobe = p%iprobe; c%idiag = p%idiag
+    c%probe_mode = p%probe_mode
+    call put(c%prefix, p%prefix)
     if (present(precision)) call put(c%gpu_precision, precision)
     rc = hydft_params_finalize(c)
   end function to_c_params
@@ -278,6 +310,40 @@ contains
     call check(m, hydft_gpu_compute_dt(m%h, dt))
     m%dt = dt
   end subroutine gpu_compute_dt
+
+  !> diag_t%budgets (diagnostics.f90:41-60) of the device state
+  subroutine gpu_budgets(m, mass, mom, ekin, fe)
+    class(model_gpu_t), intent(inout) :: m
+    real(rp), intent(out) :: mass, mom(3), ekin, fe
+    real(c_double) :: nmin, nmax
+    call check(m, hydft_gpu_budgets(m%h, mass, mom, ekin, fe, nmin, nmax))
+  end subroutine gpu_budgets
+
+  !> write_fields (io.f90:19-35)
+  subroutine gpu_write_fields(m, prefix)
+    class(model_gpu_t), intent(inout) :: m
+    character(len=*), intent(in) :: prefix
+    call check(m, hydft_gpu_write_fields(m%h, trim(prefix)//c_null_char))
+  end subroutine gpu_write_fields
+
+  !> resume from a field file written by write_fields
+  subroutine gpu_read_fields(m, path)
+    class(model_gpu_t), intent(inout) :: m
+    character(len=*), intent(in) :: path
+    integer(c_int64_t) :: st
+    call check(m, hydft_gpu_read_fields(m%h, trim(path)//c_null_char))
+    call check(m, hydft_gpu_get_time(m%h, m%t, m%dt, st))
+    m%step = int(st)
+  end subroutine gpu_read_fields
+
+  !> hydft_run's loop (hydft.f90:30-60) on the device, with its output files
+  subroutine gpu_run(m)
+    class(model_gpu_t), intent(inout) :: m
+    integer(c_int64_t) :: st
+    call check(m, hydft_gpu_run(m%h))
+    call check(m, hydft_gpu_get_time(m%h, m%t, m%dt, st))
+    m%step = int(st)
+  end subroutine gpu_run
 
   subroutine gpu_destroy(m)
     class(model_gpu_t), intent(inout) :: m
