@@ -586,16 +586,25 @@ def main():
     # calls with a probe of one mode read back each step (the driver's loop,
     # src/hydft.f90:41-51), the final state read back
     me = hg.Model(workload_params(hg, n, "fp32"), structure=st, device=dev)
-    host_n = np.ascontiguousarray(nin)
+
+    def pinned(shape):
+        return torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
+
+    # host state in pinned memory, as a caller that streams states would keep it
+    host_in = (pinned((n, n, n)), pinned((3, n, n, n)), pinned((6, n, n, n)))
+    host_in[0][...] = nin
+    host_in[1][...] = 0.0
+    host_in[2][...] = 0.0
+    host_out = (pinned((n, n, n)), pinned((3, n, n, n)), pinned((6, n, n, n)))
     torch.cuda.synchronize(dev)
     barrier()
     t0 = time.perf_counter()
-    me.set_state(host_n, zeros3, zeros6)
+    me.set_state(*host_in)
     me.set_time(0.0, dt)
     for _ in range(args.steps):
         me.advance(1)
         me.mode(0, 1, 0, 0)
-    fin = me.get_state()
+    fin = me.get_state(out=host_out)
     torch.cuda.synchronize(dev)
     e2e_s = time.perf_counter() - t0
     if dist is not None:
@@ -605,7 +614,9 @@ def main():
     state_bytes = 8 * (1 + 3 + 6) * cells
     e2e = {"value": cells * args.steps * world / e2e_s, "unit": UNIT,
            "h2d_bytes_per_step": state_bytes / args.steps,
-           "d2h_bytes_per_step": 16 + state_bytes / args.steps}
+           "d2h_bytes_per_step": 16 + state_bytes / args.steps,
+           "path": "set_state from pinned FP64 host arrays, per step advance(1) + one mode read "
+                   "(src/hydft.f90:41-51 with iprobe = 1), get_state into pinned arrays; wall clock"}
     me.close()
     del fin
 

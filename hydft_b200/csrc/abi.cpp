@@ -111,10 +111,7 @@ int hydft_gpu_set_state(hydft_gpu *h, const double *n, const double *mom, const 
 {
     if (!h) return HYDFT_ERR_BAD_ARG;
     cudaSetDevice(h->device);
-    const size_t nc = (size_t)h->mh.p.nx * h->mh.p.ny * h->mh.p.nz;
-    if (n)
-        for (size_t q = 0; q < nc; ++q)
-            if (!(n[q] > 0.0)) return fail(h, HYDFT_ERR_NONPOSITIVE_DENSITY, "initial density is not positive");
+    // positivity of n is checked on the device by the solver
     return wrap(h, h->s->set_state(n, mom, pi));
 }
 

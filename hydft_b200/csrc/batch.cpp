@@ -12,11 +12,14 @@
 // the loop every member follows); this grouping has no counterpart there.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <map>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/hydft_gpu.h"
@@ -126,63 +129,118 @@ int hydft_batch_create(int n, const hydft_params *params, const hydft_structure 
     cudaSetDevice(device);
     auto b = std::make_unique<hydft_batch>();
     b->device = device;
+    // Members are built on several host threads (the setup kernels run on
+    // each thread's own default stream, so the HNC solves of different
+    // members overlap on the device).  Members whose HNC inputs agree share
+    // one solve: one member per distinct input is built first, the others
+    // then take its structure table.
+    std::vector<hydft_gpu *> hs(n, nullptr);
+    std::vector<int> rcs(n, 0);
+    std::vector<std::string> errs(n);
+    std::vector<std::string> keys(n);
+    std::map<std::string, int> first;   // key -> the member that solves it
+    std::vector<int> wave1, wave2;
+    for (int i = 0; i < n; ++i) {
+        keys[i] = hnc_key(params[i]);
+        const bool given = structures && structures[i].n > 0;
+        const bool hnc = std::string(params[i].structure) == "hnc";
+        if (!given && hnc) {
+            auto it = first.find(keys[i]);
+            if (it == first.end()) {
+                first[keys[i]] = i;
+                wave1.push_back(i);
+            } else {
+                wave2.push_back(i);
+            }
+        } else {
+            wave1.push_back(i);
+        }
+    }
     std::map<std::string, CachedStructure> cache;
+    auto build = [&](int i, const hydft_structure *sp) {
+        cudaSetDevice(device);
+        rcs[i] = hydft_gpu_create(&params[i], sp, device, &hs[i]);
+        if (rcs[i]) errs[i] = hydft_gpu_create_error();
+    };
+    auto run_wave = [&](const std::vector<int> &wave, bool cached) {
+        const int nth = std::max(1, std::min<int>((int)wave.size(), std::min(16u, std::max(1u, std::thread::hardware_concurrency()))));
+        std::atomic<int> next{0};
+        auto worker = [&]() {
+            for (int w; (w = next.fetch_add(1)) < (int)wave.size();) {
+                const int i = wave[w];
+                hydft_structure st{};
+                const hydft_structure *sp = nullptr;
+                if (structures && structures[i].n > 0) {
+                    sp = &structures[i];
+                } else if (cached) {
+                    const CachedStructure &c = cache.at(keys[i]);
+                    st.n = (int)c.k.size();
+                    st.k = c.k.data();
+                    st.c = c.c.data();
+                    st.u_ex = c.u_ex;
+                    st.du_dgamma = c.du_dgamma;
+                    st.has_energy = c.has_energy;
+                    sp = &st;
+                }
+                build(i, sp);
+            }
+        };
+        std::vector<std::thread> ths;
+        for (int k = 0; k < nth; ++k) ths.emplace_back(worker);
+        for (auto &th : ths) th.join();
+    };
     auto cleanup = [&]() {
+        for (auto *h : hs) destroy_member(h);
+    };
+    auto first_error = [&]() -> int {
+        for (int i = 0; i < n; ++i)
+            if (rcs[i]) {
+                cleanup();
+                set_thread_error("member " + std::to_string(i) + ": " + errs[i]);
+                return rcs[i];
+            }
+        return 0;
+    };
+    run_wave(wave1, false);
+    if (int rc = first_error()) return rc;
+    for (auto &kv : first) {
+        const hydft_gpu *h = hs[kv.second];
+        if (!h->mh.has_st) continue;
+        CachedStructure c;
+        c.k = h->mh.st_k;
+        c.c = h->mh.st_c;
+        c.u_ex = h->mh.u_ex;
+        c.du_dgamma = h->mh.du_dgamma;
+        c.has_energy = h->mh.has_energy ? 1 : 0;
+        cache[kv.first] = std::move(c);
+    }
+    // a key whose first member found no table: the others solve themselves
+    std::vector<int> cached2, solve2;
+    for (int i : wave2) (cache.count(keys[i]) ? cached2 : solve2).push_back(i);
+    run_wave(cached2, true);
+    run_wave(solve2, false);
+    if (int rc = first_error()) return rc;
+    for (int i = 0; i < n; ++i) {
+        hs[i]->owned_by_batch = true;
+        b->m.push_back(hs[i]);
+    }
+    auto cleanup_members = [&]() {
         for (auto *h : b->m) destroy_member(h);
         b->m.clear();
     };
-    for (int i = 0; i < n; ++i) {
-        const hydft_params &p = params[i];
-        hydft_structure st{};
-        const hydft_structure *sp = nullptr;
-        const bool given = structures && structures[i].n > 0;
-        const std::string key = hnc_key(p);
-        const bool hnc = std::string(p.structure) == "hnc";
-        if (given) {
-            sp = &structures[i];
-        } else if (hnc && cache.count(key)) {
-            const CachedStructure &c = cache[key];
-            st.n = (int)c.k.size();
-            st.k = c.k.data();
-            st.c = c.c.data();
-            st.u_ex = c.u_ex;
-            st.du_dgamma = c.du_dgamma;
-            st.has_energy = c.has_energy;
-            sp = &st;
-        }
-        hydft_gpu *h = nullptr;
-        int rc = hydft_gpu_create(&p, sp, device, &h);
-        if (rc) {
-            const std::string msg = "member " + std::to_string(i) + ": " + hydft_gpu_create_error();
-            cleanup();
-            set_thread_error(msg);
-            return rc;
-        }
-        h->owned_by_batch = true;
-        b->m.push_back(h);
-        if (!given && hnc && !cache.count(key) && h->mh.has_st) {
-            CachedStructure c;
-            c.k = h->mh.st_k;
-            c.c = h->mh.st_c;
-            c.u_ex = h->mh.u_ex;
-            c.du_dgamma = h->mh.du_dgamma;
-            c.has_energy = h->mh.has_energy ? 1 : 0;
-            cache[key] = std::move(c);
-        }
-    }
     cudaSetDevice(device);
     if (cudaStreamCreateWithFlags(&b->root, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) != cudaSuccess ||
         cudaMallocHost(&b->hstat, sizeof(unsigned) * n) != cudaSuccess) {
-        cleanup();
+        cleanup_members();
         set_thread_error("ensemble: stream, event or pinned buffer creation failed");
         return HYDFT_ERR_CUDA;
     }
     b->join.resize(n);
     for (int i = 0; i < n; ++i)
         if (cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming) != cudaSuccess) {
-            cleanup();
+            cleanup_members();
             set_thread_error("ensemble: event creation failed");
             return HYDFT_ERR_CUDA;
         }

@@ -281,6 +281,40 @@ static __global__ void gauss_force_final_kernel(const double *part, int nb, Ctrl
     }
 }
 
+// FP64 compensated sum, minimum and count of non-finite values of x[0..n)
+// per block, into part[block * NSUM + 0 / 1 / 2]
+static __global__ void density_stats_kernel(const double *x, size_t n, double *part)
+{
+    double a = 0.0, c = 0.0, mn = 1e300, bad = 0.0;
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const double v = x[q];
+        if (!isfinite(v)) bad += 1.0;
+        neumaier<double>(a, c, v);
+        mn = fmin(mn, v);
+    }
+    __shared__ double sh[3][8];
+    double s = a + c;
+    for (int off = 16; off > 0; off >>= 1) {
+        s += __shfl_down_sync(0xffffffffu, s, off);
+        mn = fmin(mn, __shfl_down_sync(0xffffffffu, mn, off));
+        bad += __shfl_down_sync(0xffffffffu, bad, off);
+    }
+    const int w = threadIdx.x / 32, l = threadIdx.x % 32;
+    if (l == 0) { sh[0][w] = s; sh[1][w] = mn; sh[2][w] = bad; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0, tc = 0.0, m = 1e300, b = 0.0;
+        for (int j = 0; j < (int)(blockDim.x / 32); ++j) {
+            neumaier<double>(t, tc, sh[0][j]);
+            m = fmin(m, sh[1][j]);
+            b += sh[2][j];
+        }
+        part[blockIdx.x * NSUM + 0] = t + tc;
+        part[blockIdx.x * NSUM + 1] = m;
+        part[blockIdx.x * NSUM + 2] = b;
+    }
+}
+
 template <typename R>
 __global__ void fill_real_kernel(R *dst, const double *src, double sub, size_t n)
 {
@@ -1377,16 +1411,35 @@ public:
     {
         if (!n || !mom) { err = "set_state: n and mom are required"; return HYDFT_E_BAD; }
         if (ph.evolve && !pi) { err = "set_state: pi is required for the Maxwell closure"; return HYDFT_E_BAD; }
-        // mean density in FP64 (the k = 0 mode), deviations transformed in R
-        double s = 0.0, c = 0.0;
-        for (size_t q = 0; q < ncell; ++q) {
-            const double v = n[q];
+        // the density in FP64 on the device: its mean (the k = 0 mode, kept
+        // exactly; the deviations are transformed in R), minimum and
+        // non-finite count
+        double *tmp;
+        CK(cudaMallocAsync((void **)&tmp, ncell * sizeof(double), st));
+        CK(cudaMemcpyAsync(tmp, n, ncell * sizeof(double), cudaMemcpyHostToDevice, st));
+        density_stats_kernel<<<red_blocks, 256, 0, st>>>(tmp, ncell, spart);
+        launches++;
+        std::vector<double> hp((size_t)red_blocks * NSUM);
+        CK(cudaMemcpyAsync(hp.data(), spart, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        double s = 0.0, c = 0.0, nmin = 1e300, bad = 0.0;
+        for (int b = 0; b < red_blocks; ++b) {
+            const double v = hp[(size_t)b * NSUM];
             const double t = s + v;
             if (std::fabs(s) >= std::fabs(v)) c += (s - t) + v; else c += (v - t) + s;
             s = t;
+            nmin = std::min(nmin, hp[(size_t)b * NSUM + 1]);
+            bad += hp[(size_t)b * NSUM + 2];
+        }
+        if (bad > 0.0 || !(nmin > 0.0)) {
+            cudaFreeAsync(tmp, st);
+            err = "initial density is not positive";
+            return HYDFT_E_NONPOS;
         }
         const double nmean = (s + c) / (double)ncell;
-        if (int rc = up(io_real, n, 1, nmean)) return rc;
+        fill_real_kernel<R><<<592, 256, 0, st>>>(io_real, tmp, nmean, ncell);
+        launches++;
+        CK(cudaFreeAsync(tmp, st));
         if (int rc = up(io_real + ncell, mom, 3, 0.0)) return rc;
         const R *src[4] = {io_real, io_real + ncell, io_real + 2 * ncell, io_real + 3 * ncell};
         cplx<R> *dst[4] = {N, M[0], M[1], M[2]};

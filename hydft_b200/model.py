@@ -241,10 +241,17 @@ class Model:
             pi = None
         self._check(lib().hydft_gpu_set_state(self.h, _ptr(n), _ptr(mom), _ptr(pi)))
 
-    def get_state(self):
-        n = np.zeros(self.shape)
-        mom = np.zeros((3,) + self.shape)
-        pi = np.zeros((6,) + self.shape) if self.has_pi else None
+    def get_state(self, out=None):
+        """(n, mom, pi) as host arrays; `out` may supply the arrays to fill
+        (C-contiguous float64, e.g. pinned buffers)."""
+        if out is None:
+            n = np.zeros(self.shape)
+            mom = np.zeros((3,) + self.shape)
+            pi = np.zeros((6,) + self.shape) if self.has_pi else None
+        else:
+            n, mom, pi = out
+            if not self.has_pi:
+                pi = None
         self._check(lib().hydft_gpu_get_state(self.h, _ptr(n), _ptr(mom), _ptr(pi)))
         return n, mom, pi
 

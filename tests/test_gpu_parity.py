@@ -240,6 +240,20 @@ def test_initial_conditions(hg, orc):
     assert rel(m.n, m.scalar("n0") * (1 + 0.02 * d)) < 1e-13
 
 
+def test_set_state_rejects_a_nonpositive_density(hg):
+    m = hg.Model(hg.default_params(dt=0.5, **CASES["ion_newtonian_3d"]))
+    n = np.full(m.shape, m.scalar("n0"))
+    n[3, 2, 1] = 0.0
+    with pytest.raises(hg.HydftError) as e:
+        m.set_state(n)
+    assert e.value.code == 3
+    n[3, 2, 1] = np.nan
+    with pytest.raises(hg.HydftError) as e:
+        m.set_state(n)
+    assert e.value.code == 3
+    m.close()
+
+
 def test_nonpositive_density_is_an_error(hg):
     m = hg.Model(hg.default_params(dt=0.5, **CASES["ion_1d"]))
     n0 = m.scalar("n0")
