@@ -384,7 +384,7 @@ double footprint_bytes(const hydft_params *pin)
     const int ninB = nm + (evolve ? 6 * nm : 0), noutB = nm + (evolve ? 6 : 0);
     const int nin = std::max({ninA, ninB, 10}), nout = std::max({noutA, noutB, 10});
     double bytes = cb * (68.0 * csize + nin * zsize + (p.ny > 1 ? nin * ysize : 0.0) + nout * ysize) +
-                   b * (14.0 * ncell + csize);
+                   b * (14.0 * ncell + csize) + 8.0 * ncell;   // + the FP64 staging field
     const std::string terms = p.terms;
     if (terms.find("hartree") != std::string::npos) bytes += b * csize;   // v(k) for the energy
     if (terms.find("ry") != std::string::npos) bytes += b * csize;        // c_cor(k) for the energy

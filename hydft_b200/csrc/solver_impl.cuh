@@ -402,6 +402,7 @@ public:
     R *gV = nullptr, *gG = nullptr;        // gaussian potential and its gradient (3 fields), real space
     cplx<R> *Vg = nullptr;                 // gaussian potential on the band
     double *spart = nullptr, *sout = nullptr;   // block partials and results of the 6-sum reductions
+    double *stage = nullptr;                    // one FP64 field: host copies pass through it
     double *pring = nullptr;                    // probe records (5 doubles each)
     int *pcount = nullptr;
     long long pidx = -1;
@@ -569,6 +570,7 @@ public:
         if (int rc = alloc(dn_real, ncell)) return rc;
         if (int rc = alloc(u_real, 3 * ncell)) return rc;
         if (int rc = alloc(io_real, 10 * ncell)) return rc;
+        if (int rc = alloc(stage, ncell)) return rc;   // FP64 staging of host fields
         CK(cudaMemset(u_real, 0, 3 * ncell * sizeof(R)));
         if (int rc = alloc(Klin, csize)) return rc;
         {
@@ -1382,28 +1384,27 @@ public:
     }
 
     // device real (R) -> host double, ncomp fields
+    // device fields (R) -> host FP64 arrays, one component at a time through
+    // the FP64 staging field
     int down(double *h, const R *d, int ncomp, double add)
     {
-        double *tmp;
-        const size_t n = ncomp * ncell;
-        CK(cudaMallocAsync((void **)&tmp, n * sizeof(double), st));
-        real_to_double_kernel<R><<<592, 256, 0, st>>>(tmp, d, add, n);
-        launches++;
-        CK(cudaMemcpyAsync(h, tmp, n * sizeof(double), cudaMemcpyDeviceToHost, st));
-        CK(cudaFreeAsync(tmp, st));
+        for (int c = 0; c < ncomp; ++c) {
+            real_to_double_kernel<R><<<592, 256, 0, st>>>(stage, d + (size_t)c * ncell, add, ncell);
+            launches++;
+            CK(cudaMemcpyAsync(h + (size_t)c * ncell, stage, ncell * sizeof(double), cudaMemcpyDeviceToHost, st));
+        }
         CK(cudaStreamSynchronize(st));
         return 0;
     }
 
+    // host FP64 arrays -> device fields (R) minus `sub`, through the staging field
     int up(R *d, const double *h, int ncomp, double sub)
     {
-        double *tmp;
-        const size_t n = ncomp * ncell;
-        CK(cudaMallocAsync((void **)&tmp, n * sizeof(double), st));
-        CK(cudaMemcpyAsync(tmp, h, n * sizeof(double), cudaMemcpyHostToDevice, st));
-        fill_real_kernel<R><<<592, 256, 0, st>>>(d, tmp, sub, n);
-        launches++;
-        CK(cudaFreeAsync(tmp, st));
+        for (int c = 0; c < ncomp; ++c) {
+            CK(cudaMemcpyAsync(stage, h + (size_t)c * ncell, ncell * sizeof(double), cudaMemcpyHostToDevice, st));
+            fill_real_kernel<R><<<592, 256, 0, st>>>(d + (size_t)c * ncell, stage, sub, ncell);
+            launches++;
+        }
         return 0;
     }
 
@@ -1414,10 +1415,8 @@ public:
         // the density in FP64 on the device: its mean (the k = 0 mode, kept
         // exactly; the deviations are transformed in R), minimum and
         // non-finite count
-        double *tmp;
-        CK(cudaMallocAsync((void **)&tmp, ncell * sizeof(double), st));
-        CK(cudaMemcpyAsync(tmp, n, ncell * sizeof(double), cudaMemcpyHostToDevice, st));
-        density_stats_kernel<<<red_blocks, 256, 0, st>>>(tmp, ncell, spart);
+        CK(cudaMemcpyAsync(stage, n, ncell * sizeof(double), cudaMemcpyHostToDevice, st));
+        density_stats_kernel<<<red_blocks, 256, 0, st>>>(stage, ncell, spart);
         launches++;
         std::vector<double> hp((size_t)red_blocks * NSUM);
         CK(cudaMemcpyAsync(hp.data(), spart, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -1432,14 +1431,12 @@ public:
             bad += hp[(size_t)b * NSUM + 2];
         }
         if (bad > 0.0 || !(nmin > 0.0)) {
-            cudaFreeAsync(tmp, st);
             err = "initial density is not positive";
             return HYDFT_E_NONPOS;
         }
         const double nmean = (s + c) / (double)ncell;
-        fill_real_kernel<R><<<592, 256, 0, st>>>(io_real, tmp, nmean, ncell);
+        fill_real_kernel<R><<<592, 256, 0, st>>>(io_real, stage, nmean, ncell);
         launches++;
-        CK(cudaFreeAsync(tmp, st));
         if (int rc = up(io_real + ncell, mom, 3, 0.0)) return rc;
         const R *src[4] = {io_real, io_real + ncell, io_real + 2 * ncell, io_real + 3 * ncell};
         cplx<R> *dst[4] = {N, M[0], M[1], M[2]};

@@ -92,5 +92,5 @@ def test_footprint_of_the_256_maxwell_step():
     f64 = hg.footprint(hg.default_params(gpu_precision="fp64", **kw))
     newt = hg.footprint(hg.default_params(gpu_precision="fp32", **dict(kw, closure="newtonian")))
     assert 3.5e9 < f32 < 5.0e9
-    assert abs(f64 / f32 - 2.0) < 0.01
+    assert 1.9 < f64 / f32 < 2.0      # everything doubles but the FP64 staging field
     assert newt < f32
