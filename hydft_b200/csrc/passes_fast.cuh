@@ -18,6 +18,63 @@ namespace hydft {
 __device__ __forceinline__ int fft_signed(int n, int L) { return n <= L / 2 ? n : n - L; }
 
 // ------------------------------------------------------------ y/z passes
+// Column element addressing with 32-bit offsets from a per-thread base: a
+// column of length L has its elements `rs` array elements apart.
+//
+// Band layout (the compact axis of the spectral arrays): signed index m
+// with |m| <= M stored at c = m (m >= 0) or m + nc (m < 0); the thread's
+// stride-layout elements are n = t + T e, so the offset of element e is
+// (t or t - L + nc) * rs + e * T * rs and lies in the band when n <= M or
+// n >= L - M.
+template <typename R, int T, int E>
+__device__ __forceinline__ void load_band(cplx<R> (&v)[E], const cplx<R> *__restrict__ col, int rs, int t, int M,
+                                          int nc, bool valid)
+{
+    constexpr int L = T * E;
+    const int lo_off = t * rs, hi_off = (t - L + nc) * rs, step = T * rs;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int n = t + T * e;
+        const bool lo = n <= M, hi = n >= L - M;
+        const int off = (lo ? lo_off : hi_off) + e * step;
+        v[e] = (valid && (lo || hi)) ? col[off] : cplx<R>{R(0), R(0)};
+    }
+}
+
+template <typename R, int T, int E>
+__device__ __forceinline__ void store_band(cplx<R> *__restrict__ col, const cplx<R> (&v)[E], int rs, int t, int M,
+                                           int nc, R scale)
+{
+    constexpr int L = T * E;
+    const int lo_off = t * rs, hi_off = (t - L + nc) * rs, step = T * rs;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int n = t + T * e;
+        const bool lo = n <= M, hi = n >= L - M;
+        if (lo || hi) col[(lo ? lo_off : hi_off) + e * step] = scale * v[e];
+    }
+}
+
+// Full layout, block order: register r holds position block_pos(t, r)
+template <typename R, int T, int E>
+__device__ __forceinline__ void load_block(cplx<R> (&v)[E], const cplx<R> *__restrict__ col, int rs, int t, bool valid)
+{
+    const int base = t * rs;
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+        const int off = base + (T * (r / T) + E * (r % T)) * rs;
+        v[r] = valid ? col[off] : cplx<R>{R(0), R(0)};
+    }
+}
+
+template <typename R, int T, int E>
+__device__ __forceinline__ void store_block(cplx<R> *__restrict__ col, const cplx<R> (&v)[E], int rs, int t)
+{
+    const int base = t * rs;
+#pragma unroll
+    for (int r = 0; r < E; ++r) col[base + (T * (r / T) + E * (r % T)) * rs] = v[r];
+}
+
 template <typename R, int T, int E, int TX, int G>
 __global__ void __launch_bounds__(TX * T * G) zinv_fast(Grid g, PassArgs<R> a, const cplx<R> *twz)
 {
@@ -28,20 +85,15 @@ __global__ void __launch_bounds__(TX * T * G) zinv_fast(Grid g, PassArgs<R> a, c
     const int tid = threadIdx.x, c = tid % TX, t = (tid / TX) % T, gi = tid / (TX * T);
     const int x = blockIdx.x * TX + c, kyc = blockIdx.y * G + gi, f = blockIdx.z;
     const bool valid = x < g.nkxc && kyc < g.nkyc;
-    const cplx<R> *__restrict__ in = a.in[f];
-    cplx<R> *__restrict__ out = a.out[f];
     const int op = a.op[f];
     for (int i = tid; i < 2 * L; i += blockDim.x) tw[i] = twz[i];
     const int my = valid ? signed_idx(kyc, g.My) : 0;
     const R kx = R(x * g.kx0), ky = R(my * g.ky0);
+    // kz runs over the compact band: element stride nkyc * pkx
+    const int rs = g.nkyc * g.pkx;
+    const size_t col = (size_t)kyc * g.pkx + x;
     cplx<R> v[E];
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-        const int mz = fft_signed(t + T * e, L);
-        const bool ok = valid && mz >= -g.Mz && mz <= g.Mz;
-        const int kzc = mz >= 0 ? mz : mz + g.nkzc;
-        v[e] = ok ? in[((size_t)kzc * g.nkyc + kyc) * g.pkx + x] : cplx<R>{R(0), R(0)};
-    }
+    load_band<R, T, E>(v, a.in[f] + col, rs, t, g.Mz, g.nkzc, valid);
     // the operator is uniform over the block
     switch (op) {
     case OP_ZK0:
@@ -70,13 +122,8 @@ __global__ void __launch_bounds__(TX * T * G) zinv_fast(Grid g, PassArgs<R> a, c
     }
     __syncthreads();
     stride_to_block<T, E, +1, R, BarBlock, TX>(v, t, xb + gi * (L + L / T) * TX + c, tw);
-    if (valid) {
-#pragma unroll
-        for (int r = 0; r < E; ++r) {
-            const int z = block_pos<T, E>(t, r);
-            out[((size_t)z * g.nkyc + kyc) * g.pkx + x] = v[r];
-        }
-    }
+    // z runs over the full axis: element stride nkyc * pkx in the ZI layout
+    if (valid) store_block<R, T, E>(a.out[f] + col, v, rs, t);
 }
 
 template <typename R, int T, int E, int TX, int G>
@@ -89,29 +136,12 @@ __global__ void __launch_bounds__(TX * T * G) yinv_fast(Grid g, PassArgs<R> a, c
     const int tid = threadIdx.x, c = tid % TX, t = (tid / TX) % T, gi = tid / (TX * T);
     const int x = blockIdx.x * TX + c, z = blockIdx.y * G + gi, f = blockIdx.z;
     const bool valid = x < g.nkxc && z < g.nz;
-    const cplx<R> *__restrict__ in = a.in[f];
-    cplx<R> *__restrict__ out = a.out[f];
     for (int i = tid; i < 2 * L; i += blockDim.x) tw[i] = twy[i];
     cplx<R> v[E];
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-        const int my = fft_signed(t + T * e, L);
-        cplx<R> val = {R(0), R(0)};
-        if (valid && my >= -g.My && my <= g.My) {
-            const int kyc = my >= 0 ? my : my + g.nkyc;
-            val = in[((size_t)z * g.nkyc + kyc) * g.pkx + x];
-        }
-        v[e] = val;
-    }
+    load_band<R, T, E>(v, a.in[f] + (size_t)z * g.nkyc * g.pkx + x, g.pkx, t, g.My, g.nkyc, valid);
     __syncthreads();
     stride_to_block<T, E, +1, R, BarBlock, TX>(v, t, xb + gi * (L + L / T) * TX + c, tw);
-    if (valid) {
-#pragma unroll
-        for (int r = 0; r < E; ++r) {
-            const int y = block_pos<T, E>(t, r);
-            out[((size_t)z * g.ny + y) * g.pkx + x] = v[r];
-        }
-    }
+    if (valid) store_block<R, T, E>(a.out[f] + (size_t)z * g.ny * g.pkx + x, v, g.pkx, t);
 }
 
 template <typename R, int T, int E, int TX, int G>
@@ -124,27 +154,12 @@ __global__ void __launch_bounds__(TX * T * G) yfwd_fast(Grid g, PassArgs<R> a, c
     const int tid = threadIdx.x, c = tid % TX, t = (tid / TX) % T, gi = tid / (TX * T);
     const int x = blockIdx.x * TX + c, z = blockIdx.y * G + gi, f = blockIdx.z;
     const bool valid = x < g.nkxc && z < g.nz;
-    const cplx<R> *__restrict__ in = a.in[f];
-    cplx<R> *__restrict__ out = a.out[f];
     for (int i = tid; i < 2 * L; i += blockDim.x) tw[i] = twy[i];
     cplx<R> v[E];
-#pragma unroll
-    for (int r = 0; r < E; ++r) {
-        const int y = block_pos<T, E>(t, r);
-        v[r] = valid ? in[((size_t)z * g.ny + y) * g.pkx + x] : cplx<R>{R(0), R(0)};
-    }
+    load_block<R, T, E>(v, a.in[f] + (size_t)z * g.ny * g.pkx + x, g.pkx, t, valid);
     __syncthreads();
     block_to_stride<T, E, -1, R, BarBlock, TX>(v, t, xb + gi * (L + L / T) * TX + c, tw);
-    if (valid) {
-#pragma unroll
-        for (int m = 0; m < E; ++m) {
-            const int my = fft_signed(t + T * m, L);
-            if (my >= -g.My && my <= g.My) {
-                const int kyc = my >= 0 ? my : my + g.nkyc;
-                out[((size_t)z * g.nkyc + kyc) * g.pkx + x] = v[m];
-            }
-        }
-    }
+    if (valid) store_band<R, T, E>(a.out[f] + (size_t)z * g.nkyc * g.pkx + x, v, g.pkx, t, g.My, g.nkyc, R(1));
 }
 
 template <typename R, int T, int E, int TX, int G>
@@ -157,27 +172,14 @@ __global__ void __launch_bounds__(TX * T * G) zfwd_fast(Grid g, PassArgs<R> a, c
     const int tid = threadIdx.x, c = tid % TX, t = (tid / TX) % T, gi = tid / (TX * T);
     const int x = blockIdx.x * TX + c, kyc = blockIdx.y * G + gi, f = blockIdx.z;
     const bool valid = x < g.nkxc && kyc < g.nkyc;
-    const cplx<R> *__restrict__ in = a.in[f];
-    cplx<R> *__restrict__ out = a.out[f];
     for (int i = tid; i < 2 * L; i += blockDim.x) tw[i] = twz[i];
+    const int rs = g.nkyc * g.pkx;
+    const size_t col = (size_t)kyc * g.pkx + x;
     cplx<R> v[E];
-#pragma unroll
-    for (int r = 0; r < E; ++r) {
-        const int z = block_pos<T, E>(t, r);
-        v[r] = valid ? in[((size_t)z * g.nkyc + kyc) * g.pkx + x] : cplx<R>{R(0), R(0)};
-    }
+    load_block<R, T, E>(v, a.in[f] + col, rs, t, valid);
     __syncthreads();
     block_to_stride<T, E, -1, R, BarBlock, TX>(v, t, xb + gi * (L + L / T) * TX + c, tw);
-    if (valid) {
-#pragma unroll
-        for (int m = 0; m < E; ++m) {
-            const int mz = fft_signed(t + T * m, L);
-            if (mz >= -g.Mz && mz <= g.Mz) {
-                const int kzc = mz >= 0 ? mz : mz + g.nkzc;
-                out[((size_t)kzc * g.nkyc + kyc) * g.pkx + x] = norm * v[m];
-            }
-        }
-    }
+    if (valid) store_band<R, T, E>(a.out[f] + col, v, rs, t, g.Mz, g.nkzc, norm);
 }
 
 // smem bytes of a y/z fast pass
