@@ -86,6 +86,8 @@ int capture(hydft_batch *b)
 {
     drop_graph(b);
     const size_t n = b->m.size();
+    for (size_t i = 0; i < n; ++i)
+        if (int rc = b->m[i]->s->prepare()) return fail(b, rc, "member " + std::to_string(i) + ": " + b->m[i]->s->err);
     std::vector<int64_t> before(n);
     for (size_t i = 0; i < n; ++i) before[i] = b->m[i]->s->launches;
     cudaError_t e = cudaStreamBeginCapture(b->root, cudaStreamCaptureModeThreadLocal);

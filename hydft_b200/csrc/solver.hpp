@@ -76,6 +76,11 @@ public:
     // launching a graph or synchronising (an ensemble captures the steps of
     // many solvers into one graph through this call).
     virtual void enqueue_steps(int k) = 0;
+    // picks the tile shapes (autotuner) if not done yet; must precede a
+    // capture of enqueue_steps
+    virtual int prepare() = 0;
+    // tile shapes in use: kx columns per y/z block, threads per x block
+    virtual void tiles(int *yz, int *xnt) const = 0;
     // records that steps enqueued earlier (a replayed ensemble graph) ran
     virtual void mark_advanced() = 0;
     // k replays of the captured step graph on this solver's stream, without

@@ -18,6 +18,9 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -418,6 +421,10 @@ public:
     bool host_pending = false;   // a Maxwell relaxation waits for u of the new state
     bool fast_x = false;         // x passes on the register FFT (3-D grids, planned nx)
     bool staged_x = true;        // xa_regs / xb_rows (HYDFT_XPASS=v1 selects xa_fast / xb_fast)
+    // tile shapes picked by tune(): kx columns per y/z block, threads per x block
+    int yz_tx = sizeof(R) == 4 ? 16 : 8;
+    int x_ntmax = 256;
+    bool tuned = false;
     size_t alloc_bytes = 0;      // device memory allocated by this solver
     int num_sms = 148;
 
@@ -715,6 +722,14 @@ public:
     // inverse transform of nf spectral fields (with load-time operators) into
     // YI buffers 0..nf-1
     static constexpr int YZ_TX = sizeof(R) == 4 ? 16 : 8;
+
+    // the y/z passes' kx columns per block (8 or 16) as a compile-time constant
+    template <class F>
+    void with_tx(F &&f) const
+    {
+        if (yz_tx == 8) f(std::integral_constant<int, 8>{});
+        else f(std::integral_constant<int, 16>{});
+    }
     static constexpr int YZ_NT = sizeof(R) == 4 ? 256 : 128;
 
     template <class K>
@@ -736,13 +751,16 @@ public:
         }
         const double zbytes = nf * cb() * g.nkxc * g.nkyc * (double)(g.nkzc + g.nz);
         const bool zf = with_plan(g.nz, [&](auto Tc, auto Ec) {
-            constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value, TX = YZ_TX;
+            constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value;
+            with_tx([&](auto TXc) {
+            constexpr int TX = decltype(TXc)::value;
             constexpr int G = YZ_NT / (TX * T) > 0 ? YZ_NT / (TX * T) : 1;
             const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
             auto k = zinv_fast<R, T, E, TX, G>;
             set_smem(k, sm);
             const dim3 grid((g.nkxc + TX - 1) / TX, (g.nkyc + G - 1) / G, nf);
             launch("zinv", zbytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, a, tpz); });
+            });
         });
         if (!zf) {
             const int ntx = (g.nkxc + TX - 1) / TX;
@@ -759,13 +777,16 @@ public:
             }
             const double ybytes = nf * cb() * g.nkxc * g.nz * (double)(g.nkyc + g.ny);
             const bool yf = with_plan(g.ny, [&](auto Tc, auto Ec) {
-                constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value, TX = YZ_TX;
+                constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value;
+                with_tx([&](auto TXc) {
+                constexpr int TX = decltype(TXc)::value;
                 constexpr int G = YZ_NT / (TX * T) > 0 ? YZ_NT / (TX * T) : 1;
                 const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
                 auto k = yinv_fast<R, T, E, TX, G>;
                 set_smem(k, sm);
                 const dim3 grid((g.nkxc + TX - 1) / TX, (g.nz + G - 1) / G, nf);
                 launch("yinv", ybytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, b, tpy); });
+            });
             });
             if (!yf) {
                 const int ntx = (g.nkxc + TX - 1) / TX;
@@ -790,13 +811,16 @@ public:
             }
             const double ybytes = nf * cb() * g.nkxc * g.nz * (double)(g.nkyc + g.ny);
             const bool yf = with_plan(g.ny, [&](auto Tc, auto Ec) {
-                constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value, TX = YZ_TX;
+                constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value;
+                with_tx([&](auto TXc) {
+                constexpr int TX = decltype(TXc)::value;
                 constexpr int G = YZ_NT / (TX * T) > 0 ? YZ_NT / (TX * T) : 1;
                 const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
                 auto k = yfwd_fast<R, T, E, TX, G>;
                 set_smem(k, sm);
                 const dim3 grid((g.nkxc + TX - 1) / TX, (g.nz + G - 1) / G, nf);
                 launch("yfwd", ybytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, b, tpy); });
+            });
             });
             if (!yf) {
                 const size_t smy = sizeof(cplx<R>) * (2 * (size_t)g.ny * TX + g.ny);
@@ -814,13 +838,16 @@ public:
         const R norm = R(1.0 / ((double)g.nx * g.ny * g.nz));
         const double zbytes = nf * cb() * g.nkxc * g.nkyc * (double)(g.nkzc + g.nz);
         const bool zf = with_plan(g.nz, [&](auto Tc, auto Ec) {
-            constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value, TX = YZ_TX;
+            constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value;
+            with_tx([&](auto TXc) {
+            constexpr int TX = decltype(TXc)::value;
             constexpr int G = YZ_NT / (TX * T) > 0 ? YZ_NT / (TX * T) : 1;
             const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
             auto k = zfwd_fast<R, T, E, TX, G>;
             set_smem(k, sm);
             const dim3 grid((g.nkxc + TX - 1) / TX, (g.nkyc + G - 1) / G, nf);
             launch("zfwd", zbytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, a, tpz, norm); });
+            });
         });
         if (!zf) {
             const size_t smz = sizeof(cplx<R>) * (2 * (size_t)g.nz * TX + g.nz);
@@ -833,7 +860,7 @@ public:
     template <int T, int E>
     int x_threads(int np_slots, size_t &smem) const
     {
-        int nt = 256;
+        int nt = x_ntmax;
         for (;;) {
             smem = sizeof(cplx<R>) * (2 * (size_t)T * E + (size_t)(nt / T) * xrow_stride<T, E>() + (size_t)np_slots * E * nt) +
                    (np_slots ? 2 * sizeof(R) * (size_t)E * nt : 0);
@@ -873,7 +900,7 @@ public:
                 launch(name, xbytes(nin, nout, nreal), [&] { k<<<(nrows + rb - 1) / rb, nt, sm, st>>>(g, a, tpx, pw); });
             };
             auto go_regs = [&](auto k) {
-                const int nt = 256 / T * T;
+                const int nt = std::min(256, x_ntmax) / T * T;
                 const size_t sm = xstaged_smem<R, T, E>(nt, g.pkx, 0, 0);
                 set_smem(k, sm);
                 const int rb = nt / T;
@@ -908,7 +935,7 @@ public:
                 launch("xpass_b", xbytes(nin, nout, nreal), [&] { k<<<(nrows + rb - 1) / rb, nt, sm, st>>>(g, a, tpx, pw); });
             };
             auto go_rows = [&](auto k, int nreal_rows) {
-                int nt = 256 / T * T;
+                int nt = std::min(256, x_ntmax) / T * T;
                 size_t sm = xstaged_smem<R, T, E>(nt, g.pkx, 2, nreal_rows);
                 // two blocks per SM: 228 KB of shared memory, 1 KB reserved per block
                 while (sm > 115712 && nt > T) {
@@ -1194,6 +1221,14 @@ public:
 
     const unsigned *status_word() const override { return &ctrl->status; }
 
+    int prepare() override { return tune(); }
+
+    void tiles(int *yz, int *xnt) const override
+    {
+        *yz = yz_tx;
+        *xnt = x_ntmax;
+    }
+
     void enqueue_steps(int k) override
     {
         for (int i = 0; i < k; ++i) one_step();
@@ -1280,8 +1315,123 @@ public:
 
     size_t device_bytes() const override { return alloc_bytes; }
 
+    // Autotuner of the tile shapes: times the phase-B transform sequence
+    // (y/z inverse of its inputs, x pass B, y/z forward of its outputs) with
+    // each candidate shape on the current data, writing only work buffers,
+    // and keeps the fastest.  Every shape gives the same results to the bit
+    // (the same arithmetic per element, only the blocking differs).  The
+    // choice is shared by every model of the same grid, precision and
+    // physics in the process.  HYDFT_TUNE=0 keeps the defaults.
+    struct TuneKey {
+        int nx, ny, nz, bytes, nm, evolve, ext;
+        bool operator<(const TuneKey &o) const
+        {
+            return std::tie(nx, ny, nz, bytes, nm, evolve, ext) < std::tie(o.nx, o.ny, o.nz, o.bytes, o.nm, o.evolve, o.ext);
+        }
+    };
+    static std::map<TuneKey, std::pair<int, int>> &tune_cache()
+    {
+        static std::map<TuneKey, std::pair<int, int>> m;
+        return m;
+    }
+    static std::mutex &tune_mutex()
+    {
+        static std::mutex m;
+        return m;
+    }
+
+    int tune()
+    {
+        if (tuned) return 0;
+        tuned = true;
+        const char *ev = std::getenv("HYDFT_TUNE");
+        if (ev && std::string(ev) == "0") return 0;
+        // fixed shapes on request (HYDFT_YZ_TILE = 8 | 16, HYDFT_X_THREADS = 128 | 256)
+        const char *fy = std::getenv("HYDFT_YZ_TILE"), *fx = std::getenv("HYDFT_X_THREADS");
+        if ((fy && *fy) || (fx && *fx)) {
+            if (fy && (std::string(fy) == "8" || std::string(fy) == "16")) yz_tx = std::atoi(fy);
+            if (fx && (std::string(fx) == "128" || std::string(fx) == "256")) x_ntmax = std::atoi(fx);
+            return 0;
+        }
+        if (!(has_plan(g.ny) || has_plan(g.nz))) return 0;
+        const TuneKey key{g.nx, g.ny, g.nz, (int)sizeof(R), nm, ph.evolve, ph.ext_active ? ph.ext_kind : 0};
+        {
+            std::lock_guard<std::mutex> lk(tune_mutex());
+            auto it = tune_cache().find(key);
+            if (it != tune_cache().end()) {
+                yz_tx = it->second.first;
+                x_ntmax = it->second.second;
+                return 0;
+            }
+        }
+        // the phase-B pass sequence of stage 0
+        const cplx<R> *src[MAXF];
+        int ops[MAXF];
+        int nf = 0;
+        for (int d = 0; d < nm; ++d) { src[nf] = MU; ops[nf++] = OP_IKX + d; }
+        if (ph.evolve)
+            for (int cp = 0; cp < 3; ++cp)
+                for (int d = 0; d < nm; ++d)
+                    for (int h = 0; h < 2; ++h) { src[nf] = P[2 * cp + h]; ops[nf++] = OP_IKX + d; }
+        const int nout = nm + (ph.evolve ? 6 : 0);
+        PWB<R> pw;
+        pw.ph = ph;
+        pw.nm = nm;
+        pw.nhat = N;
+        pw.dn_real = dn_real;
+        pw.u_real = u_real;
+        pw.ncell = ncell;
+        pw.ex = ex; pw.ey = ey; pw.ez = ez;
+        pw.gradv = gG;
+        pw.ctrl = ctrl;
+        pw.stage = 0;
+        pw.status = &ctrl->status;
+        const int64_t launches0 = launches;
+        cudaEvent_t e0, e1;
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        auto time_it = [&](int tx, int ntmax) -> float {
+            yz_tx = tx;
+            x_ntmax = ntmax;
+            float best = 1e30f;
+            for (int rep = 0; rep < 3; ++rep) {
+                cudaEventRecord(e0, st);
+                inverse(nf, src, ops);
+                if (fast_x) xb_launch(nf, nout, pw, ph.evolve ? 1 + nm : 1);
+                else xpass(nf, nout, pw, xrb_b, "xpass_b", ph.evolve ? 1 + nm : 1);
+                forward(nout, OB);
+                cudaEventRecord(e1, st);
+                cudaEventSynchronize(e1);
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (rep > 0) best = std::min(best, ms);   // the first run warms up
+            }
+            return best;
+        };
+        const int txs[2] = {8, 16};
+        const int nts[2] = {128, 256};
+        float best = 1e30f;
+        int btx = yz_tx, bnt = x_ntmax;
+        for (int tx : txs)
+            for (int nt : nts) {
+                if (!fast_x && nt != 256) continue;
+                const float ms = time_it(tx, nt);
+                if (ms < best) { best = ms; btx = tx; bnt = nt; }
+            }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        launches = launches0;
+        yz_tx = btx;
+        x_ntmax = bnt;
+        CK(cudaGetLastError());
+        std::lock_guard<std::mutex> lk(tune_mutex());
+        tune_cache()[key] = {btx, bnt};
+        return 0;
+    }
+
     int launch_steps(int nsteps) override
     {
+        if (int rc = tune()) return rc;
         if (nsteps <= 0) return 0;
         if (!gexec) {
             const int64_t before = launches;

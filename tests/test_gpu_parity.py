@@ -286,3 +286,34 @@ def test_free_energy_matches_oracle(hg, orc, case):
     fe = m.budgets()[3]
     ofe = o.budgets()[3]
     assert abs(fe - ofe) <= TOL64 * max(abs(ofe), 1e-300)
+
+
+def test_tile_shapes_give_identical_results(hg, monkeypatch):
+    """The autotuner's candidate tile shapes (kx columns per y/z block, threads
+    per x block) only change the blocking: every shape gives the same fields
+    to the bit, and the tuned model keeps one of the candidates."""
+    kw = dict(ION, nx=64, ny=32, nz=48, lx=32.0, ly=16.0, lz=24.0, closure="maxwell", tau_model="constant",
+              tau=1.5, dt=0.01, gpu_precision="fp32")
+    out = []
+    for tile, nt in (("8", "128"), ("16", "256"), ("8", "256")):
+        monkeypatch.setenv("HYDFT_YZ_TILE", tile)
+        monkeypatch.setenv("HYDFT_X_THREADS", nt)
+        m = hg.Model(hg.default_params(**kw))
+        n, mom, pi = seeded_state(m)
+        m.set_state(n, mom, pi)
+        m.advance(3)
+        assert m.scalar("yz_tile") == int(tile) and m.scalar("x_threads") == int(nt)
+        out.append(m.get_state())
+        m.close()
+    for other in out[1:]:
+        for x, y in zip(out[0], other):
+            assert np.array_equal(x, y)
+    monkeypatch.delenv("HYDFT_YZ_TILE")
+    monkeypatch.delenv("HYDFT_X_THREADS")
+    m = hg.Model(hg.default_params(**kw))
+    n, mom, pi = seeded_state(m)
+    m.set_state(n, mom, pi)
+    m.advance(3)
+    assert m.scalar("yz_tile") in (8, 16) and m.scalar("x_threads") in (128, 256)
+    for x, y in zip(m.get_state(), out[0]):
+        assert np.array_equal(x, y)
