@@ -282,6 +282,7 @@ struct Ctrl {
     // amplitude and exp(-i omega t) of that time
     double v_amp, v_ewr, v_ewi;
     double gf[3];            // mean of n F_ext for the gaussian potential, stage start
+    double nmean;            // mean density in FP64 (conserved; the k = 0 mode of n)
 };
 
 // physics constants for the pointwise and spectral kernels
@@ -304,7 +305,8 @@ template <typename R>
 struct PWA {
     Phys ph;
     int nm;
-    const cplx<R> *nhat;       // compact n, element 0 = mean density
+    const cplx<R> *nhat;       // compact n
+    const double *nmean;       // the mean density in FP64
     const double *fdtab;
     R *dn_real;                // real-space dn for phase B
     R *u_real;                 // real-space u (3 fields) when Pi evolves
@@ -313,7 +315,7 @@ struct PWA {
 
     __device__ void operator()(const Grid &g, int row, int x, const R *Fin, R *Fout, int stride) const
     {
-        const double nref = (double)nhat[0].x;
+        const double nref = *nmean;
         const R dn = Fin[0];
         const double n = nref + (double)dn;
         const size_t q = (size_t)row * g.nx + x;
@@ -373,6 +375,7 @@ struct PWB {
     Phys ph;
     int nm;
     const cplx<R> *nhat;
+    const double *nmean;       // the mean density in FP64
     const R *dn_real, *u_real;
     size_t ncell;
     const cplx<double> *ex, *ey, *ez;   // exp(i k_d x_d) per axis
@@ -384,7 +387,7 @@ struct PWB {
     __device__ void operator()(const Grid &g, int row, int x, const R *Fin, R *Fout, int stride) const
     {
         const size_t q = (size_t)row * g.nx + x;
-        const double nref = (double)nhat[0].x;
+        const double nref = *nmean;
         const R n = R(nref + (double)dn_real[q]);
         R f[3] = {R(0), R(0), R(0)};
         if (ph.ext_active && ph.ext_kind == 3) {
@@ -419,10 +422,11 @@ struct PWU {
     Phys ph;
     int nm;
     const cplx<R> *nhat;
+    const double *nmean;       // the mean density in FP64
     unsigned *status;
     __device__ void operator()(const Grid &g, int row, int x, const R *Fin, R *Fout, int stride) const
     {
-        const double n = (double)nhat[0].x + (double)Fin[0];
+        const double n = *nmean + (double)Fin[0];
         if (!(n > 0.0)) atomicOr(status, isfinite(n) ? ST_NONPOS : ST_NONFINITE);
         const R inv_mn = R(1.0 / (ph.mass * n));
         for (int d = 0; d < nm; ++d) Fout[d * stride] = Fin[(1 + d) * stride] * inv_mn;

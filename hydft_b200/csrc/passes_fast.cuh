@@ -312,7 +312,8 @@ __global__ void __launch_bounds__(256, HYDFT_XMINB) xa_fast(Grid g, XFastArgs<R>
     };
     // the mean density is exact in the k = 0 mode; deviations carry the
     // signal, so n, 1/(m n) and ln(n/nref) are formed in the field precision
-    const R nref = pw.nhat[0].x;
+    const double nref64 = *pw.nmean;
+    const R nref = R(nref64);
     const R inv_nref = R(1) / nref, inv_beta = R(pw.ph.inv_beta), mass = R(pw.ph.mass);
     const size_t rowbase = (size_t)row * g.nx;
     // density check, real-space dn and u for phase B, 1/(m n) and the local
@@ -341,7 +342,7 @@ __global__ void __launch_bounds__(256, HYDFT_XMINB) xa_fast(Grid g, XFastArgs<R>
                     mu += log1p(dn * inv_nref) * inv_beta;
                 } else {
                     // alpha(n) by FP64 Newton on the Fermi-Dirac table
-                    const double n64 = (double)nref + (double)dn;
+                    const double n64 = nref64 + (double)dn;
                     any64 = true;
                     if (!have_alpha) {
                         bool ok = true;
@@ -405,7 +406,8 @@ __global__ void __launch_bounds__(256, HYDFT_XMINB) xb_fast(Grid g, XFastArgs<R>
     cplx<R> *xrow = xbuf + rr * xrow_stride<T, E>();
     for (int i = tid; i < 2 * L; i += nt) tw[i] = twx[i];
     __syncthreads();
-    const R nref = pw.nhat[0].x;
+    const double nref64 = *pw.nmean;
+    const R nref = R(nref64);
     const size_t rowbase = (size_t)row * g.nx;
     const int y = rowok ? row % g.ny : 0, z = rowok ? row / g.ny : 0;
     // n (dmu - F): pairs of components
@@ -545,7 +547,8 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xa_regs(Grid g, XFa
     cplx<R> p0[E], p1[E];   // (dn, m_0), (m_1, m_2)
     x_c2r_pair<R, T, E>(p0, a.in[0], a.in[1], row, rowok, t, g, xrow, tw);
     x_c2r_pair<R, T, E>(p1, a.in[2], a.in[3], row, rowok, t, g, xrow, tw);
-    const R nref = pw.nhat[0].x;
+    const double nref64 = *pw.nmean;
+    const R nref = R(nref64);
     const R inv_nref = R(1) / nref, inv_beta = R(pw.ph.inv_beta), mass = R(pw.ph.mass);
     const size_t rowbase = (size_t)row * g.nx;
     // mu_local (ideal terms in the given order) and 1/(m n); p0[r].x becomes 1/(m n)
@@ -683,7 +686,8 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xb_rows(Grid g, XFa
         stage(p + 1);
         pf.upto((fb >= 0 ? fb : fa) + 2 + AHEAD);
     };
-    const R nref = pw.nhat[0].x;
+    const double nref64 = *pw.nmean;
+    const R nref = R(nref64);
     const int y = rowok ? row % g.ny : 0, z = rowok ? row / g.ny : 0;
     // n (dmu - F): pairs of components
 #pragma unroll

@@ -61,11 +61,11 @@ __device__ __forceinline__ void neumaier(double &s, double &c, double v)
 // FP64 compensated sums of n, m_d, m_d^2/n and extrema over the real-space
 // fields; one partial per block, combined in a fixed order by reduce_final.
 template <typename R>
-__global__ void reduce_fields_kernel(const R *dn, const R *m, size_t ncell, int nm, const cplx<R> *nhat,
+__global__ void reduce_fields_kernel(const R *dn, const R *m, size_t ncell, int nm, const double *nmean,
                                      double inv_mass, RedPart *part)
 {
     __shared__ RedPart sh[8];
-    const double nref = (double)nhat[0].x;
+    const double nref = *nmean;
     RedPart p;
     p.sn = p.cn_ = p.sk = p.ck = 0.0;
     for (int d = 0; d < 3; ++d) p.sm[d] = p.cm[d] = 0.0;
@@ -641,6 +641,7 @@ public:
             c.v_amp = (s.ext_td && s.ext_ramp > 0.0) ? 0.0 : s.ext_amp;
             c.v_ewr = 1.0;
             c.v_ewi = 0.0;
+            c.nmean = s.n0;
             CK(cudaMemcpy(ctrl, &c, sizeof(c), cudaMemcpyHostToDevice));
         }
         red_blocks = 2 * 148;
@@ -1017,6 +1018,7 @@ public:
         pw.ph = ph;
         pw.nm = nm;
         pw.nhat = N;
+        pw.nmean = &ctrl->nmean;
         pw.fdtab = fdtab;
         pw.dn_real = dn_real;
         pw.u_real = write_u ? u_real : nullptr;
@@ -1057,6 +1059,7 @@ public:
         pw.ph = ph;
         pw.nm = nm;
         pw.nhat = N;
+        pw.nmean = &ctrl->nmean;
         pw.dn_real = dn_real;
         pw.u_real = u_real;
         pw.ncell = ncell;
@@ -1128,6 +1131,7 @@ public:
             pa.ph = ph;
             pa.nm = nm;
             pa.nhat = N;
+            pa.nmean = &ctrl->nmean;
             pa.fdtab = fdtab;
             pa.dn_real = nullptr;
             pa.u_real = nullptr;
@@ -1139,6 +1143,7 @@ public:
             pw.ph = ph;
             pw.nm = nm;
             pw.nhat = N;
+        pw.nmean = &ctrl->nmean;
             pw.status = &ctrl->status;
             xpass(nf, nm, pw, xrb_io, "xpass_u");
         }
@@ -1378,6 +1383,7 @@ public:
         pw.ph = ph;
         pw.nm = nm;
         pw.nhat = N;
+        pw.nmean = &ctrl->nmean;
         pw.dn_real = dn_real;
         pw.u_real = u_real;
         pw.ncell = ncell;
@@ -1593,6 +1599,7 @@ public:
         if (int rc = from_real(4, src, dst)) return rc;
         set_k0_kernel<R><<<1, 32, 0, st>>>(N, nmean);
         launches++;
+        CK(cudaMemcpyAsync(&ctrl->nmean, &nmean, sizeof(double), cudaMemcpyHostToDevice, st));
         if (ph.evolve) {
             if (int rc = up(io_real, pi, 6, 0.0)) return rc;
             const R *sp[6];
@@ -1611,10 +1618,8 @@ public:
         finish_if_pending();
         double nmean = 0.0;
         {
-            cplx<R> h0;
-            CK(cudaMemcpyAsync(&h0, N, sizeof(h0), cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(&nmean, &ctrl->nmean, sizeof(double), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
-            nmean = (double)h0.x;
         }
         const cplx<R> *src[MAXF];
         R *dsts[MAXF];
@@ -1655,7 +1660,7 @@ public:
         for (int d = 0; d < nm; ++d) pw.dst[1 + d] = io_real + (1 + d) * ncell;
         pw.ncell = ncell;
         x_toreal(1 + nm, pw);
-        reduce_fields_kernel<R><<<red_blocks, 256, 0, st>>>(io_real, io_real + ncell, ncell, nm, N,
+        reduce_fields_kernel<R><<<red_blocks, 256, 0, st>>>(io_real, io_real + ncell, ncell, nm, &ctrl->nmean,
                                                             ph.inv_mass, rpart);
         reduce_final_kernel<R><<<1, 32, 0, st>>>(rpart, red_blocks, rout);
         launches += 2;
@@ -1685,10 +1690,9 @@ public:
         if (ph.has_grad && nm < 3)
             CK(cudaMemsetAsync(io_real + (size_t)(1 + nm) * ncell, 0, (3 - nm) * ncell * sizeof(R), st));
         x_toreal(1 + ngr, pw);
-        cplx<R> h0;
-        CK(cudaMemcpyAsync(&h0, N, sizeof(h0), cudaMemcpyDeviceToHost, st));
+        double nmean = 0.0;
+        CK(cudaMemcpyAsync(&nmean, &ctrl->nmean, sizeof(double), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
-        const double nmean = (double)h0.x;
         double spec[NSUM], real[NSUM];
         energy_spec_kernel<R><<<red_blocks, 256, 0, st>>>(g, N, Kh, Kr, spart);
         sums_final_kernel<<<1, 32, 0, st>>>(spart, red_blocks, sout);
@@ -1743,6 +1747,13 @@ public:
         mz = g.nz > 1 ? wrapm(mz, g.nz) : 0;
         if (mx > g.Mx || std::abs(my) > g.My || std::abs(mz) > g.Mz) {
             *re = 0.0;
+            *im = 0.0;
+            return 0;
+        }
+        if (field == 0 && mx == 0 && my == 0 && mz == 0) {
+            // the mean density, kept in FP64
+            CK(cudaMemcpyAsync(re, &ctrl->nmean, sizeof(double), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
             *im = 0.0;
             return 0;
         }
