@@ -329,6 +329,7 @@ int hydft_gpu_get_scalar(const hydft_gpu *h, const char *name, double *v)
         h->s->tiles(&yz, &xn);
         *v = k == "yz_tile" ? yz : xn;
     }
+    else if (k == "band_axes") *v = h->s->band_axes();
     else if (k == "ext_omega") *v = m.ext_omega;
     else if (k == "hnc_niter") *v = m.hnc_niter;
     else if (k == "wmax") *v = m.wmax;

@@ -457,12 +457,17 @@ struct PWFromReal {
 };
 
 // ---------------------------------------------------- spectral combines
+// mode index -> (kx, ky, kz) compact indices.  The band holds fewer than
+// 2^31 modes (the solver refuses larger grids), so the split uses 32-bit
+// unsigned division: a 64-bit divide is a long software sequence per mode.
 __host__ __device__ __forceinline__ void kvec(const Grid &g, size_t idx, int &kxc, int &kyc, int &kzc)
 {
-    kxc = (int)(idx % g.pkx);
-    const size_t r = idx / g.pkx;
-    kyc = (int)(r % g.nkyc);
-    kzc = (int)(r / g.nkyc);
+    const unsigned i = (unsigned)idx, px = (unsigned)g.pkx, ny = (unsigned)g.nkyc;
+    const unsigned r = i / px;
+    kxc = (int)(i - r * px);
+    const unsigned z = r / ny;
+    kyc = (int)(r - z * ny);
+    kzc = (int)z;
 }
 
 template <typename R>

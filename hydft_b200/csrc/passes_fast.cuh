@@ -26,32 +26,68 @@ __device__ __forceinline__ int fft_signed(int n, int L) { return n <= L / 2 ? n 
 // stride-layout elements are n = t + T e, so the offset of element e is
 // (t or t - L + nc) * rs + e * T * rs and lies in the band when n <= M or
 // n >= L - M.
-template <typename R, int T, int E>
-__device__ __forceinline__ void load_band(cplx<R> (&v)[E], const cplx<R> *__restrict__ col, int rs, int t, int M,
+// With BAND the band limit is the two-thirds rule's M = (L - 1) / 3, a
+// compile-time constant: the elements e whose n = t + T e is in the low
+// half (n <= M), in the high half (n >= L - M) or outside the band for every
+// thread t < T are classified at compile time, so they need no per-element
+// test, and the ones outside the band are neither loaded nor stored.  Only
+// the (at most two) elements that straddle an edge keep a runtime test.
+template <int T, int E>
+__host__ __device__ constexpr int band_m() { return (T * E - 1) / 3; }
+template <int T, int E>
+__host__ __device__ constexpr bool band_all_lo(int e) { return T * e + T - 1 <= band_m<T, E>(); }
+template <int T, int E>
+__host__ __device__ constexpr bool band_all_hi(int e) { return T * e >= T * E - band_m<T, E>(); }
+template <int T, int E>
+__host__ __device__ constexpr bool band_none(int e)
+{
+    return T * e > band_m<T, E>() && T * e + T - 1 < T * E - band_m<T, E>();
+}
+
+template <typename R, int T, int E, bool BAND>
+__device__ __forceinline__ void load_band(cplx<R> (&v)[E], const cplx<R> *__restrict__ col, int rs, int t, int Mrt,
                                           int nc, bool valid)
 {
     constexpr int L = T * E;
+    const int M = BAND ? band_m<T, E>() : Mrt;
     const int lo_off = t * rs, hi_off = (t - L + nc) * rs, step = T * rs;
+    const cplx<R> zero = {R(0), R(0)};
 #pragma unroll
     for (int e = 0; e < E; ++e) {
-        const int n = t + T * e;
-        const bool lo = n <= M, hi = n >= L - M;
-        const int off = (lo ? lo_off : hi_off) + e * step;
-        v[e] = (valid && (lo || hi)) ? col[off] : cplx<R>{R(0), R(0)};
+        if (BAND && band_none<T, E>(e)) {
+            v[e] = cplx<R>{R(-0.0), R(-0.0)};
+        } else if (BAND && band_all_lo<T, E>(e)) {
+            v[e] = valid ? col[lo_off + e * step] : zero;
+        } else if (BAND && band_all_hi<T, E>(e)) {
+            v[e] = valid ? col[hi_off + e * step] : zero;
+        } else {
+            const int n = t + T * e;
+            const bool lo = n <= M, hi = n >= L - M;
+            const int off = (lo ? lo_off : hi_off) + e * step;
+            v[e] = (valid && (lo || hi)) ? col[off] : zero;
+        }
     }
 }
 
-template <typename R, int T, int E>
-__device__ __forceinline__ void store_band(cplx<R> *__restrict__ col, const cplx<R> (&v)[E], int rs, int t, int M,
+template <typename R, int T, int E, bool BAND>
+__device__ __forceinline__ void store_band(cplx<R> *__restrict__ col, const cplx<R> (&v)[E], int rs, int t, int Mrt,
                                            int nc, R scale)
 {
     constexpr int L = T * E;
+    const int M = BAND ? band_m<T, E>() : Mrt;
     const int lo_off = t * rs, hi_off = (t - L + nc) * rs, step = T * rs;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
-        const int n = t + T * e;
-        const bool lo = n <= M, hi = n >= L - M;
-        if (lo || hi) col[(lo ? lo_off : hi_off) + e * step] = scale * v[e];
+        if (BAND && band_none<T, E>(e)) continue;
+        if (BAND && band_all_lo<T, E>(e)) {
+            col[lo_off + e * step] = scale * v[e];
+        } else if (BAND && band_all_hi<T, E>(e)) {
+            col[hi_off + e * step] = scale * v[e];
+        } else {
+            const int n = t + T * e;
+            const bool lo = n <= M, hi = n >= L - M;
+            if (lo || hi) col[(lo ? lo_off : hi_off) + e * step] = scale * v[e];
+        }
     }
 }
 
@@ -75,7 +111,7 @@ __device__ __forceinline__ void store_block(cplx<R> *__restrict__ col, const cpl
     for (int r = 0; r < E; ++r) col[base + (T * (r / T) + E * (r % T)) * rs] = v[r];
 }
 
-template <typename R, int T, int E, int TX, int G>
+template <typename R, int T, int E, int TX, int G, bool BAND>
 __global__ void __launch_bounds__(TX * T * G) zinv_fast(Grid g, PassArgs<R> a, const cplx<R> *twz)
 {
     constexpr int L = T * E;
@@ -93,7 +129,7 @@ __global__ void __launch_bounds__(TX * T * G) zinv_fast(Grid g, PassArgs<R> a, c
     const int rs = g.nkyc * g.pkx;
     const size_t col = (size_t)kyc * g.pkx + x;
     cplx<R> v[E];
-    load_band<R, T, E>(v, a.in[f] + col, rs, t, g.Mz, g.nkzc, valid);
+    load_band<R, T, E, BAND>(v, a.in[f] + col, rs, t, g.Mz, g.nkzc, valid);
     // the operator is uniform over the block
     switch (op) {
     case OP_ZK0:
@@ -101,19 +137,23 @@ __global__ void __launch_bounds__(TX * T * G) zinv_fast(Grid g, PassArgs<R> a, c
         break;
     case OP_IKX:
 #pragma unroll
-        for (int e = 0; e < E; ++e) v[e] = ik_times(kx, v[e]);
+        for (int e = 0; e < E; ++e)
+            if (!(BAND && band_none<T, E>(e))) v[e] = ik_times(kx, v[e]);
         break;
     case OP_IKY:
 #pragma unroll
-        for (int e = 0; e < E; ++e) v[e] = ik_times(ky, v[e]);
+        for (int e = 0; e < E; ++e)
+            if (!(BAND && band_none<T, E>(e))) v[e] = ik_times(ky, v[e]);
         break;
     case OP_IKZ:
 #pragma unroll
-        for (int e = 0; e < E; ++e) v[e] = ik_times(R(fft_signed(t + T * e, L) * g.kz0), v[e]);
+        for (int e = 0; e < E; ++e)
+            if (!(BAND && band_none<T, E>(e))) v[e] = ik_times(R(fft_signed(t + T * e, L) * g.kz0), v[e]);
         break;
     case OP_NK2:
 #pragma unroll
         for (int e = 0; e < E; ++e) {
+            if (BAND && band_none<T, E>(e)) continue;
             const R kz = R(fft_signed(t + T * e, L) * g.kz0);
             v[e] = R(-(kx * kx + ky * ky + kz * kz)) * v[e];
         }
@@ -126,7 +166,7 @@ __global__ void __launch_bounds__(TX * T * G) zinv_fast(Grid g, PassArgs<R> a, c
     if (valid) store_block<R, T, E>(a.out[f] + col, v, rs, t);
 }
 
-template <typename R, int T, int E, int TX, int G>
+template <typename R, int T, int E, int TX, int G, bool BAND>
 __global__ void __launch_bounds__(TX * T * G) yinv_fast(Grid g, PassArgs<R> a, const cplx<R> *twy)
 {
     constexpr int L = T * E;
@@ -138,13 +178,13 @@ __global__ void __launch_bounds__(TX * T * G) yinv_fast(Grid g, PassArgs<R> a, c
     const bool valid = x < g.nkxc && z < g.nz;
     for (int i = tid; i < 2 * L; i += blockDim.x) tw[i] = twy[i];
     cplx<R> v[E];
-    load_band<R, T, E>(v, a.in[f] + (size_t)z * g.nkyc * g.pkx + x, g.pkx, t, g.My, g.nkyc, valid);
+    load_band<R, T, E, BAND>(v, a.in[f] + (size_t)z * g.nkyc * g.pkx + x, g.pkx, t, g.My, g.nkyc, valid);
     __syncthreads();
     stride_to_block<T, E, +1, R, BarBlock, TX>(v, t, xb + gi * (L + L / T) * TX + c, tw);
     if (valid) store_block<R, T, E>(a.out[f] + (size_t)z * g.ny * g.pkx + x, v, g.pkx, t);
 }
 
-template <typename R, int T, int E, int TX, int G>
+template <typename R, int T, int E, int TX, int G, bool BAND>
 __global__ void __launch_bounds__(TX * T * G) yfwd_fast(Grid g, PassArgs<R> a, const cplx<R> *twy)
 {
     constexpr int L = T * E;
@@ -159,10 +199,10 @@ __global__ void __launch_bounds__(TX * T * G) yfwd_fast(Grid g, PassArgs<R> a, c
     load_block<R, T, E>(v, a.in[f] + (size_t)z * g.ny * g.pkx + x, g.pkx, t, valid);
     __syncthreads();
     block_to_stride<T, E, -1, R, BarBlock, TX>(v, t, xb + gi * (L + L / T) * TX + c, tw);
-    if (valid) store_band<R, T, E>(a.out[f] + (size_t)z * g.nkyc * g.pkx + x, v, g.pkx, t, g.My, g.nkyc, R(1));
+    if (valid) store_band<R, T, E, BAND>(a.out[f] + (size_t)z * g.nkyc * g.pkx + x, v, g.pkx, t, g.My, g.nkyc, R(1));
 }
 
-template <typename R, int T, int E, int TX, int G>
+template <typename R, int T, int E, int TX, int G, bool BAND>
 __global__ void __launch_bounds__(TX * T * G) zfwd_fast(Grid g, PassArgs<R> a, const cplx<R> *twz, R norm)
 {
     constexpr int L = T * E;
@@ -179,7 +219,7 @@ __global__ void __launch_bounds__(TX * T * G) zfwd_fast(Grid g, PassArgs<R> a, c
     load_block<R, T, E>(v, a.in[f] + col, rs, t, valid);
     __syncthreads();
     block_to_stride<T, E, -1, R, BarBlock, TX>(v, t, xb + gi * (L + L / T) * TX + c, tw);
-    if (valid) store_band<R, T, E>(a.out[f] + col, v, rs, t, g.Mz, g.nkzc, norm);
+    if (valid) store_band<R, T, E, BAND>(a.out[f] + col, v, rs, t, g.Mz, g.nkzc, norm);
 }
 
 // smem bytes of a y/z fast pass
@@ -198,45 +238,60 @@ __host__ __device__ constexpr int xrow_stride() { return (T * E + E + 15) / 16 *
 
 // c2r input of a pair of half spectra (kx <= Mx, XF/YI layout) in stride
 // layout, then inverse FFT to block layout: v[r] = a(x) + i b(x) at
-// x = block_pos(t, r).  inb may be null (b = 0).
-template <typename R, int T, int E>
+// x = block_pos(t, r).  inb may be null (b = 0).  BAND: Mx is the
+// two-thirds rule's band_m (see load_band).
+template <typename R, int T, int E, bool BAND = false>
 __device__ __forceinline__ void x_c2r_load(cplx<R> (&v)[E], const cplx<R> *__restrict__ ina,
-                                           const cplx<R> *__restrict__ inb, size_t base, bool rowok, int t, int Mx)
+                                           const cplx<R> *__restrict__ inb, size_t base, bool rowok, int t, int Mrt)
 {
     constexpr int L = T * E;
+    const int Mx = BAND ? band_m<T, E>() : Mrt;
+    const cplx<R> zero = {R(0), R(0)};
+    // k <= Mx: a_k + i b_k; k >= L - Mx: conj(a_{L-k}) + i conj(b_{L-k})
+    auto lo = [&](int k) {
+        cplx<R> va = ina[base + k];
+        cplx<R> vb = inb ? inb[base + k] : zero;
+        if (k == 0) { va.y = R(0); vb.y = R(0); }
+        return cplx<R>{va.x - vb.y, va.y + vb.x};
+    };
+    auto hi = [&](int k) {
+        const int kk = L - k;
+        const cplx<R> va = ina[base + kk];
+        const cplx<R> vb = inb ? inb[base + kk] : zero;
+        return cplx<R>{va.x + vb.y, -va.y + vb.x};
+    };
 #pragma unroll
     for (int e = 0; e < E; ++e) {
         const int k = t + T * e;
-        cplx<R> Z = {R(0), R(0)};
-        if (rowok) {
-            if (k <= Mx) {
-                cplx<R> va = ina[base + k];
-                cplx<R> vb = inb ? inb[base + k] : cplx<R>{R(0), R(0)};
-                if (k == 0) { va.y = R(0); vb.y = R(0); }
-                Z = cplx<R>{va.x - vb.y, va.y + vb.x};
-            } else if (k >= L - Mx) {
-                const int kk = L - k;
-                cplx<R> va = ina[base + kk];
-                cplx<R> vb = inb ? inb[base + kk] : cplx<R>{R(0), R(0)};
-                Z = cplx<R>{va.x + vb.y, -va.y + vb.x};
+        if (BAND && band_none<T, E>(e)) {
+            v[e] = cplx<R>{R(-0.0), R(-0.0)};
+        } else if (BAND && band_all_lo<T, E>(e)) {
+            v[e] = rowok ? lo(k) : zero;
+        } else if (BAND && band_all_hi<T, E>(e)) {
+            v[e] = rowok ? hi(k) : zero;
+        } else {
+            cplx<R> Z = zero;
+            if (rowok) {
+                if (k <= Mx) Z = lo(k);
+                else if (k >= L - Mx) Z = hi(k);
             }
+            v[e] = Z;
         }
-        v[e] = Z;
     }
 }
 
-template <typename R, int T, int E>
+template <typename R, int T, int E, bool BAND = false>
 __device__ __forceinline__ void x_c2r_pair(cplx<R> (&v)[E], const cplx<R> *__restrict__ ina,
                                            const cplx<R> *__restrict__ inb, int row, bool rowok, int t,
                                            const Grid &g, cplx<R> *xrow, const cplx<R> *tw)
 {
-    x_c2r_load<R, T, E>(v, ina, inb, (size_t)row * g.pkx, rowok, t, g.Mx);
+    x_c2r_load<R, T, E, BAND>(v, ina, inb, (size_t)row * g.pkx, rowok, t, g.Mx);
     stride_to_block<T, E, +1, R, BarWarp, 1>(v, t, xrow, tw);
 }
 
 // r2c of z = a + i b given in block layout; writes the half spectra of a
 // and b for kx <= Mx (outb may be null)
-template <typename R, int T, int E>
+template <typename R, int T, int E, bool BAND = false>
 __device__ __forceinline__ void x_r2c_pair(cplx<R> (&v)[E], cplx<R> *__restrict__ outa, cplx<R> *__restrict__ outb,
                                            int row, bool rowok, int t, const Grid &g, cplx<R> *xrow,
                                            const cplx<R> *tw)
@@ -247,13 +302,15 @@ __device__ __forceinline__ void x_r2c_pair(cplx<R> (&v)[E], cplx<R> *__restrict_
     for (int m = 0; m < E; ++m) xrow[t + m * (T + 1)] = v[m];   // element t + T m
     __syncwarp();
     const size_t base = (size_t)row * g.pkx;
+    auto put = [&](int k) {
+        const cplx<R> zk = xrow[xidx<T>(k)];
+        const cplx<R> zm = conj(xrow[xidx<T>(k == 0 ? 0 : L - k)]);
+        outa[base + k] = R(0.5) * (zk + zm);
+        if (outb) outb[base + k] = mul_i<-1>(R(0.5) * (zk - zm));
+    };
     if (rowok) {
-        for (int k = t; k <= g.Mx; k += T) {
-            const cplx<R> zk = xrow[xidx<T>(k)];
-            const cplx<R> zm = conj(xrow[xidx<T>(k == 0 ? 0 : L - k)]);
-            outa[base + k] = R(0.5) * (zk + zm);
-            if (outb) outb[base + k] = mul_i<-1>(R(0.5) * (zk - zm));
-        }
+        const int Mx = BAND ? band_m<T, E>() : g.Mx;
+        for (int k = t; k <= Mx; k += T) put(k);
     }
     __syncwarp();
 }
@@ -525,7 +582,7 @@ __host__ __device__ constexpr int xstaged_minb() { return sizeof(R) == 4 && E <=
 // blocks fit on an SM.  The output pairs are ordered so that dn is consumed
 // first: (mu_local, u_0), (u_1, u_2), (m0u0, m0u1), (m0u2, m1u1), (m1u2, m2u2);
 // UONLY: (u_0, u_1), (u_2, -).  Outputs go to the same fields as xa_fast's.
-template <typename R, int T, int E, bool UONLY>
+template <typename R, int T, int E, bool UONLY, bool BAND>
 __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xa_regs(Grid g, XFastArgs<R> a, const cplx<R> *twx, PWA<R> pw)
 {
     constexpr int L = T * E;
@@ -545,8 +602,8 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xa_regs(Grid g, XFa
     for (int i = tid; i < 2 * L; i += nt) tw[i] = twx[i];
     __syncthreads();
     cplx<R> p0[E], p1[E];   // (dn, m_0), (m_1, m_2)
-    x_c2r_pair<R, T, E>(p0, a.in[0], a.in[1], row, rowok, t, g, xrow, tw);
-    x_c2r_pair<R, T, E>(p1, a.in[2], a.in[3], row, rowok, t, g, xrow, tw);
+    x_c2r_pair<R, T, E, BAND>(p0, a.in[0], a.in[1], row, rowok, t, g, xrow, tw);
+    x_c2r_pair<R, T, E, BAND>(p1, a.in[2], a.in[3], row, rowok, t, g, xrow, tw);
     const double nref64 = *pw.nmean;
     const R nref = R(nref64);
     const R inv_nref = R(1) / nref, inv_beta = R(pw.ph.inv_beta), mass = R(pw.ph.mass);
@@ -580,33 +637,33 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xa_regs(Grid g, XFa
     }
     if (!UONLY) {
         // outputs: 0..2 u_d, 3..8 fluxes (00, 01, 02, 11, 12, 22), 9 mu
-        x_r2c_pair<R, T, E>(v, a.out[9], a.out[0], row, rowok, t, g, xrow, tw);
+        x_r2c_pair<R, T, E, BAND>(v, a.out[9], a.out[0], row, rowok, t, g, xrow, tw);
 #pragma unroll
         for (int r = 0; r < E; ++r) v[r] = cplx<R>{p1[r].x * p0[r].x, p1[r].y * p0[r].x};
-        x_r2c_pair<R, T, E>(v, a.out[1], a.out[2], row, rowok, t, g, xrow, tw);
+        x_r2c_pair<R, T, E, BAND>(v, a.out[1], a.out[2], row, rowok, t, g, xrow, tw);
 #pragma unroll
         for (int r = 0; r < E; ++r) {
             const R u0 = p0[r].y * p0[r].x;
             v[r] = cplx<R>{p0[r].y * u0, p0[r].y * (p1[r].x * p0[r].x)};
         }
-        x_r2c_pair<R, T, E>(v, a.out[3], a.out[4], row, rowok, t, g, xrow, tw);
+        x_r2c_pair<R, T, E, BAND>(v, a.out[3], a.out[4], row, rowok, t, g, xrow, tw);
 #pragma unroll
         for (int r = 0; r < E; ++r) {
             const R u1 = p1[r].x * p0[r].x, u2 = p1[r].y * p0[r].x;
             v[r] = cplx<R>{p0[r].y * u2, p1[r].x * u1};
         }
-        x_r2c_pair<R, T, E>(v, a.out[5], a.out[6], row, rowok, t, g, xrow, tw);
+        x_r2c_pair<R, T, E, BAND>(v, a.out[5], a.out[6], row, rowok, t, g, xrow, tw);
 #pragma unroll
         for (int r = 0; r < E; ++r) {
             const R u2 = p1[r].y * p0[r].x;
             v[r] = cplx<R>{p1[r].x * u2, p1[r].y * u2};
         }
-        x_r2c_pair<R, T, E>(v, a.out[7], a.out[8], row, rowok, t, g, xrow, tw);
+        x_r2c_pair<R, T, E, BAND>(v, a.out[7], a.out[8], row, rowok, t, g, xrow, tw);
     } else {
-        x_r2c_pair<R, T, E>(v, a.out[0], a.out[1], row, rowok, t, g, xrow, tw);
+        x_r2c_pair<R, T, E, BAND>(v, a.out[0], a.out[1], row, rowok, t, g, xrow, tw);
 #pragma unroll
         for (int r = 0; r < E; ++r) v[r] = cplx<R>{p1[r].y * p0[r].x, R(0)};
-        x_r2c_pair<R, T, E>(v, a.out[2], nullptr, row, rowok, t, g, xrow, tw);
+        x_r2c_pair<R, T, E, BAND>(v, a.out[2], nullptr, row, rowok, t, g, xrow, tw);
     }
 }
 
@@ -621,7 +678,7 @@ __host__ __device__ constexpr int xreal_stride() { return T * E + T; }
 // fields ahead.  Same inputs, outputs and arithmetic as xb_fast.  EXTK: no
 // external force (0), a plane-wave potential (1), the gaussian potential's
 // static force field (2).
-template <typename R, int T, int E, bool EVOLVE, int EXTK>
+template <typename R, int T, int E, bool EVOLVE, int EXTK, bool BAND>
 __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xb_rows(Grid g, XFastArgs<R> a, const cplx<R> *twx, PWB<R> pw)
 {
     constexpr int L = T * E, NM = 3;
@@ -681,7 +738,7 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xb_rows(Grid g, XFa
         fields(p, fa, fb);
         cp_async_wait_all();
         __syncthreads();
-        x_c2r_load<R, T, E>(v, sb, fb >= 0 ? sb + (size_t)rb * pk : nullptr, (size_t)rr * pk, rowok, t, g.Mx);
+        x_c2r_load<R, T, E, BAND>(v, sb, fb >= 0 ? sb + (size_t)rb * pk : nullptr, (size_t)rr * pk, rowok, t, g.Mx);
         __syncthreads();
         stage(p + 1);
         pf.upto((fb >= 0 ? fb : fa) + 2 + AHEAD);
@@ -715,7 +772,7 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xb_rows(Grid g, XFa
             }
             v[r] = cplx<R>{n * (v[r].x - f0), n * (v[r].y - f1)};
         }
-        x_r2c_pair<R, T, E>(v, a.out[i0], i1 < NM ? a.out[i1] : nullptr, row, rowok, t, g, xrow, tw);
+        x_r2c_pair<R, T, E, BAND>(v, a.out[i0], i1 < NM ? a.out[i1] : nullptr, row, rowok, t, g, xrow, tw);
     }
     if (EVOLVE) {
         // -u.grad Pi for component pairs (0,1), (2,3), (4,5)
@@ -733,7 +790,7 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xb_rows(Grid g, XFa
 #pragma unroll
                 for (int r = 0; r < E; ++r) acc[r] = acc[r] - urow[block_pos<T, E>(t, r)] * v[r];
             }
-            x_r2c_pair<R, T, E>(acc, a.out[NM + 2 * cp], a.out[NM + 2 * cp + 1], row, rowok, t, g, xrow, tw);
+            x_r2c_pair<R, T, E, BAND>(acc, a.out[NM + 2 * cp], a.out[NM + 2 * cp + 1], row, rowok, t, g, xrow, tw);
         }
     }
 }

@@ -81,6 +81,8 @@ public:
     virtual int prepare() = 0;
     // tile shapes in use: kx columns per y/z block, threads per x block
     virtual void tiles(int *yz, int *xnt) const = 0;
+    // axes whose passes classify band elements at compile time (x 1, y 2, z 4)
+    virtual int band_axes() const = 0;
     // records that steps enqueued earlier (a replayed ensemble graph) ran
     virtual void mark_advanced() = 0;
     // k replays of the captured step graph on this solver's stream, without

@@ -421,6 +421,10 @@ public:
     bool host_pending = false;   // a Maxwell relaxation waits for u of the new state
     bool fast_x = false;         // x passes on the register FFT (3-D grids, planned nx)
     bool staged_x = true;        // xa_regs / xb_rows (HYDFT_XPASS=v1 selects xa_fast / xb_fast)
+    // the axis's band limit is the two-thirds rule's (L - 1) / 3, so the
+    // register-FFT passes classify band elements at compile time
+    // (HYDFT_BAND=0 selects the runtime test everywhere)
+    bool band_x = false, band_y = false, band_z = false;
     // tile shapes picked by tune(): kx columns per y/z block, threads per x block
     int yz_tx = sizeof(R) == 4 ? 16 : 8;
     int x_ntmax = 256;
@@ -536,6 +540,7 @@ public:
         ph.drive_in_band = s.drive_in_band; ph.drive_idx = s.drive_idx; ph.drive_conj = s.drive_conj;
 
         csize = (size_t)g.nkzc * g.nkyc * g.pkx;
+        if (csize >= ((size_t)1 << 31)) { err = "grid too large: 2^31 or more band modes"; return HYDFT_E_BAD; }
         zsize = (size_t)g.nz * g.nkyc * g.pkx;
         ysize = (size_t)g.nz * g.ny * g.pkx;
         ncell = (size_t)g.nx * g.ny * g.nz;
@@ -668,6 +673,11 @@ public:
         {
             const char *ev = std::getenv("HYDFT_XPASS");
             if (ev && std::string(ev) == "v1") staged_x = false;
+            const char *eb = std::getenv("HYDFT_BAND");
+            const bool band_ok = !(eb && std::string(eb) == "0");
+            band_x = band_ok && g.Mx == (g.nx - 1) / 3;
+            band_y = band_ok && g.My == (g.ny - 1) / 3;
+            band_z = band_ok && g.Mz == (g.nz - 1) / 3;
             CK(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
         }
         if (s.ext_active && s.ext_kind == 3) {
@@ -757,7 +767,7 @@ public:
             constexpr int TX = decltype(TXc)::value;
             constexpr int G = YZ_NT / (TX * T) > 0 ? YZ_NT / (TX * T) : 1;
             const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
-            auto k = zinv_fast<R, T, E, TX, G>;
+            auto k = band_z ? zinv_fast<R, T, E, TX, G, true> : zinv_fast<R, T, E, TX, G, false>;
             set_smem(k, sm);
             const dim3 grid((g.nkxc + TX - 1) / TX, (g.nkyc + G - 1) / G, nf);
             launch("zinv", zbytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, a, tpz); });
@@ -783,7 +793,7 @@ public:
                 constexpr int TX = decltype(TXc)::value;
                 constexpr int G = YZ_NT / (TX * T) > 0 ? YZ_NT / (TX * T) : 1;
                 const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
-                auto k = yinv_fast<R, T, E, TX, G>;
+                auto k = band_y ? yinv_fast<R, T, E, TX, G, true> : yinv_fast<R, T, E, TX, G, false>;
                 set_smem(k, sm);
                 const dim3 grid((g.nkxc + TX - 1) / TX, (g.nz + G - 1) / G, nf);
                 launch("yinv", ybytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, b, tpy); });
@@ -817,7 +827,7 @@ public:
                 constexpr int TX = decltype(TXc)::value;
                 constexpr int G = YZ_NT / (TX * T) > 0 ? YZ_NT / (TX * T) : 1;
                 const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
-                auto k = yfwd_fast<R, T, E, TX, G>;
+                auto k = band_y ? yfwd_fast<R, T, E, TX, G, true> : yfwd_fast<R, T, E, TX, G, false>;
                 set_smem(k, sm);
                 const dim3 grid((g.nkxc + TX - 1) / TX, (g.nz + G - 1) / G, nf);
                 launch("yfwd", ybytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, b, tpy); });
@@ -844,7 +854,7 @@ public:
             constexpr int TX = decltype(TXc)::value;
             constexpr int G = YZ_NT / (TX * T) > 0 ? YZ_NT / (TX * T) : 1;
             const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
-            auto k = zfwd_fast<R, T, E, TX, G>;
+            auto k = band_z ? zfwd_fast<R, T, E, TX, G, true> : zfwd_fast<R, T, E, TX, G, false>;
             set_smem(k, sm);
             const dim3 grid((g.nkxc + TX - 1) / TX, (g.nkyc + G - 1) / G, nf);
             launch("zfwd", zbytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, a, tpz, norm); });
@@ -909,9 +919,9 @@ public:
             };
             const bool no_fd = !ph.has_tf && !ph.has_grad;
             if (staged_x && uonly) {
-                go_regs(xa_regs<R, T, E, true>);
+                go_regs(band_x ? xa_regs<R, T, E, true, true> : xa_regs<R, T, E, true, false>);
             } else if (staged_x && !grad && no_fd) {
-                go_regs(xa_regs<R, T, E, false>);
+                go_regs(band_x ? xa_regs<R, T, E, false, true> : xa_regs<R, T, E, false, false>);
             } else if (uonly) {
                 go(xa_fast<R, T, E, 3, false, true>, 2);
             } else if (grad) {
@@ -948,14 +958,22 @@ public:
                 launch("xpass_b", xbytes(nin, nout, nreal), [&] { k<<<(nrows + rb - 1) / rb, nt, sm, st>>>(g, a, tpx, pw); });
             };
             const int extk = !ph.ext_active ? 0 : (ph.ext_kind == 3 ? 2 : 1);
+            auto rows = [&](auto ev, auto ek) {
+                constexpr bool EV = decltype(ev)::value;
+                constexpr int EK = decltype(ek)::value;
+                go_rows(band_x ? xb_rows<R, T, E, EV, EK, true> : xb_rows<R, T, E, EV, EK, false>, EV ? 3 : 0);
+            };
+            using std::integral_constant;
+            using EvT = integral_constant<bool, true>;
+            using EvF = integral_constant<bool, false>;
             if (staged_x && ph.evolve) {
-                if (extk == 2) go_rows(xb_rows<R, T, E, true, 2>, 3);
-                else if (extk == 1) go_rows(xb_rows<R, T, E, true, 1>, 3);
-                else go_rows(xb_rows<R, T, E, true, 0>, 3);
+                if (extk == 2) rows(EvT{}, integral_constant<int, 2>{});
+                else if (extk == 1) rows(EvT{}, integral_constant<int, 1>{});
+                else rows(EvT{}, integral_constant<int, 0>{});
             } else if (staged_x) {
-                if (extk == 2) go_rows(xb_rows<R, T, E, false, 2>, 0);
-                else if (extk == 1) go_rows(xb_rows<R, T, E, false, 1>, 0);
-                else go_rows(xb_rows<R, T, E, false, 0>, 0);
+                if (extk == 2) rows(EvF{}, integral_constant<int, 2>{});
+                else if (extk == 1) rows(EvF{}, integral_constant<int, 1>{});
+                else rows(EvF{}, integral_constant<int, 0>{});
             } else if (ph.evolve) {
                 go(xb_fast<R, T, E, 3, true>);
             } else {
@@ -1233,6 +1251,8 @@ public:
         *yz = yz_tx;
         *xnt = x_ntmax;
     }
+
+    int band_axes() const override { return (band_x ? 1 : 0) | (band_y ? 2 : 0) | (band_z ? 4 : 0); }
 
     void enqueue_steps(int k) override
     {

@@ -317,3 +317,29 @@ def test_tile_shapes_give_identical_results(hg, monkeypatch):
     assert m.scalar("yz_tile") in (8, 16) and m.scalar("x_threads") in (128, 256)
     for x, y in zip(m.get_state(), out[0]):
         assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_band_classified_passes_match_runtime_band_test(hg, monkeypatch, prec):
+    """With the two-thirds band limit M = (L - 1) / 3 the register-FFT passes
+    classify the band elements at compile time and skip the ones outside
+    the band; the fields equal those of the passes that test every element
+    at run time (HYDFT_BAND=0).  Without dealiasing no axis qualifies."""
+    kw = dict(ION, nx=64, ny=32, nz=48, lx=32.0, ly=16.0, lz=24.0, closure="maxwell", tau_model="constant",
+              tau=1.5, dt=0.01, gpu_precision=prec)
+    out = []
+    for flag, axes in (("0", 0), ("1", 7)):
+        monkeypatch.setenv("HYDFT_BAND", flag)
+        m = hg.Model(hg.default_params(**kw))
+        assert m.scalar("band_axes") == axes
+        n, mom, pi = seeded_state(m)
+        m.set_state(n, mom, pi)
+        m.advance(3)
+        out.append(m.get_state())
+        m.close()
+    for x, y in zip(out[0], out[1]):
+        assert np.array_equal(x, y)
+    monkeypatch.delenv("HYDFT_BAND")
+    m = hg.Model(hg.default_params(**dict(kw, dealias=False)))
+    assert m.scalar("band_axes") == 0
+    m.close()
