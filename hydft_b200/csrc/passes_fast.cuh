@@ -179,6 +179,13 @@ __global__ void __launch_bounds__(TX * T * G) yinv_fast(Grid g, PassArgs<R> a, c
     for (int i = tid; i < 2 * L; i += blockDim.x) tw[i] = twy[i];
     cplx<R> v[E];
     load_band<R, T, E, BAND>(v, a.in[f] + (size_t)z * g.nkyc * g.pkx + x, g.pkx, t, g.My, g.nkyc, valid);
+    // OP_IKY: the y derivative of a field whose z transform is shared with
+    // other derivatives (k_y is constant along z); uniform over the block
+    if (a.op[f] == OP_IKY) {
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+            if (!(BAND && band_none<T, E>(e))) v[e] = ik_times(R(fft_signed(t + T * e, L) * g.ky0), v[e]);
+    }
     __syncthreads();
     stride_to_block<T, E, +1, R, BarBlock, TX>(v, t, xb + gi * (L + L / T) * TX + c, tw);
     if (valid) store_block<R, T, E>(a.out[f] + (size_t)z * g.ny * g.pkx + x, v, g.pkx, t);
@@ -240,24 +247,34 @@ __host__ __device__ constexpr int xrow_stride() { return (T * E + E + 15) / 16 *
 // layout, then inverse FFT to block layout: v[r] = a(x) + i b(x) at
 // x = block_pos(t, r).  inb may be null (b = 0).  BAND: Mx is the
 // two-thirds rule's band_m (see load_band).
+//
+// dxa / dxb: the input is differentiated along x on the way in (a_k becomes
+// i k kx0 a_k), for fields whose z and y transforms are shared with their
+// other derivatives.
 template <typename R, int T, int E, bool BAND = false>
 __device__ __forceinline__ void x_c2r_load(cplx<R> (&v)[E], const cplx<R> *__restrict__ ina,
-                                           const cplx<R> *__restrict__ inb, size_t base, bool rowok, int t, int Mrt)
+                                           const cplx<R> *__restrict__ inb, size_t base, bool rowok, int t, int Mrt,
+                                           bool dxa = false, bool dxb = false, R kx0 = R(0))
 {
     constexpr int L = T * E;
     const int Mx = BAND ? band_m<T, E>() : Mrt;
     const cplx<R> zero = {R(0), R(0)};
+    auto get = [&](int kk, cplx<R> &va, cplx<R> &vb) {
+        va = ina[base + kk];
+        vb = inb ? inb[base + kk] : zero;
+        if (dxa) va = ik_times(R(kk) * kx0, va);
+        if (dxb) vb = ik_times(R(kk) * kx0, vb);
+    };
     // k <= Mx: a_k + i b_k; k >= L - Mx: conj(a_{L-k}) + i conj(b_{L-k})
     auto lo = [&](int k) {
-        cplx<R> va = ina[base + k];
-        cplx<R> vb = inb ? inb[base + k] : zero;
+        cplx<R> va, vb;
+        get(k, va, vb);
         if (k == 0) { va.y = R(0); vb.y = R(0); }
         return cplx<R>{va.x - vb.y, va.y + vb.x};
     };
     auto hi = [&](int k) {
-        const int kk = L - k;
-        const cplx<R> va = ina[base + kk];
-        const cplx<R> vb = inb ? inb[base + kk] : zero;
+        cplx<R> va, vb;
+        get(L - k, va, vb);
         return cplx<R>{va.x + vb.y, -va.y + vb.x};
     };
 #pragma unroll
@@ -320,6 +337,7 @@ struct XFastArgs {
     const cplx<R> *in[MAXF];
     cplx<R> *out[MAXF];
     int nin, nout;
+    int dx_in_pass;   // phase B (xb_rows): the x derivatives arrive underived
 };
 
 // packed (i <= j) flux index -> (i, j) for three components
@@ -675,9 +693,11 @@ __host__ __device__ constexpr int xreal_stride() { return T * E + T; }
 // Phase B with this block's real-space rows (dn and, when Pi evolves, u_d)
 // copied into shared memory by cp.async at the start; the copies overlap the
 // first inverse transform, and the spectral inputs are prefetched to L2 a few
-// fields ahead.  Same inputs, outputs and arithmetic as xb_fast.  EXTK: no
-// external force (0), a plane-wave potential (1), the gaussian potential's
-// static force field (2).
+// fields ahead.  Same inputs, outputs and arithmetic as xb_fast, except that
+// with a.dx_in_pass the x derivatives (of mu and of each Pi component)
+// arrive underived, sharing their z and y transforms with the y derivative,
+// and are differentiated here on the way in.  EXTK: no external force (0), a
+// plane-wave potential (1), the gaussian potential's static force field (2).
 template <typename R, int T, int E, bool EVOLVE, int EXTK, bool BAND>
 __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xb_rows(Grid g, XFastArgs<R> a, const cplx<R> *twx, PWB<R> pw)
 {
@@ -733,12 +753,15 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xb_rows(Grid g, XFa
     for (int r = 0; r < E; ++r) dnv[r] = rowok ? pw.dn_real[rowbase + block_pos<T, E>(t, r)] : R(0);
     for (int i = tid; i < 2 * L; i += nt) tw[i] = twx[i];
     // the staged pair p into registers, then pair p + 1 on its way
-    auto load = [&](int p, cplx<R> (&v)[E]) {
+    const R kx0 = R(g.kx0);
+    const bool dxs = a.dx_in_pass != 0;
+    auto load = [&](int p, cplx<R> (&v)[E], bool dxa, bool dxb) {
         int fa, fb;
         fields(p, fa, fb);
         cp_async_wait_all();
         __syncthreads();
-        x_c2r_load<R, T, E, BAND>(v, sb, fb >= 0 ? sb + (size_t)rb * pk : nullptr, (size_t)rr * pk, rowok, t, g.Mx);
+        x_c2r_load<R, T, E, BAND>(v, sb, fb >= 0 ? sb + (size_t)rb * pk : nullptr, (size_t)rr * pk, rowok, t, g.Mx,
+                                  dxa, dxb, kx0);
         __syncthreads();
         stage(p + 1);
         pf.upto((fb >= 0 ? fb : fa) + 2 + AHEAD);
@@ -751,7 +774,7 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xb_rows(Grid g, XFa
     for (int q = 0; 2 * q < NM; ++q) {
         const int i0 = 2 * q, i1 = 2 * q + 1;
         cplx<R> v[E];
-        load(q, v);
+        load(q, v, dxs && q == 0, false);   // d/dx of mu
         stride_to_block<T, E, +1, R, BarWarp, 1>(v, t, xrow, tw);
 #pragma unroll
         for (int r = 0; r < E; ++r) {
@@ -784,7 +807,7 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xb_rows(Grid g, XFa
 #pragma unroll
             for (int d = 0; d < NM; ++d) {
                 cplx<R> v[E];
-                load(2 + cp * NM + d, v);
+                load(2 + cp * NM + d, v, dxs && d == 0, dxs && d == 0);   // d/dx of Pi
                 stride_to_block<T, E, +1, R, BarWarp, 1>(v, t, xrow, tw);
                 const R *urow = rs + ((size_t)d * rb + rr) * RS;
 #pragma unroll

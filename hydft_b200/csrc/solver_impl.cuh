@@ -753,14 +753,26 @@ public:
     // YI buffers 0..nf-1
     void inverse(int nf, const cplx<R> *const *src, const int *ops)
     {
+        int ysrc[MAXF], yops[MAXF];
+        for (int f = 0; f < nf; ++f) { ysrc[f] = f; yops[f] = OP_ID; }
+        inverse_shared(nf, src, ops, nf, ysrc, yops);
+    }
+
+    // inverse transform with shared z transforms: nzf spectral fields (with
+    // z-load operators) go to ZI buffers 0..nzf-1; YI buffer j is the y
+    // transform of ZI buffer ysrc[j] with the y-load operator yops[j] (OP_ID,
+    // or OP_IKY on axes with a register plan)
+    void inverse_shared(int nzf, const cplx<R> *const *src, const int *ops, int nf, const int *ysrc,
+                        const int *yops)
+    {
         PassArgs<R> a;
-        a.nf = nf;
-        for (int f = 0; f < nf; ++f) {
+        a.nf = nzf;
+        for (int f = 0; f < nzf; ++f) {
             a.in[f] = src[f];
             a.out[f] = zi + (size_t)f * zsize;
             a.op[f] = ops[f];
         }
-        const double zbytes = nf * cb() * g.nkxc * g.nkyc * (double)(g.nkzc + g.nz);
+        const double zbytes = nzf * cb() * g.nkxc * g.nkyc * (double)(g.nkzc + g.nz);
         const bool zf = with_plan(g.nz, [&](auto Tc, auto Ec) {
             constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value;
             with_tx([&](auto TXc) {
@@ -769,22 +781,22 @@ public:
             const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
             auto k = band_z ? zinv_fast<R, T, E, TX, G, true> : zinv_fast<R, T, E, TX, G, false>;
             set_smem(k, sm);
-            const dim3 grid((g.nkxc + TX - 1) / TX, (g.nkyc + G - 1) / G, nf);
+            const dim3 grid((g.nkxc + TX - 1) / TX, (g.nkyc + G - 1) / G, nzf);
             launch("zinv", zbytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, a, tpz); });
             });
         });
         if (!zf) {
             const int ntx = (g.nkxc + TX - 1) / TX;
             const size_t smz = sizeof(cplx<R>) * (2 * (size_t)g.nz * TX + g.nz);
-            launch("zinv", zbytes, [&] { zinv_kernel<R, TX><<<dim3(ntx, g.nkyc, nf), 256, smz, st>>>(g, a, twz); });
+            launch("zinv", zbytes, [&] { zinv_kernel<R, TX><<<dim3(ntx, g.nkyc, nzf), 256, smz, st>>>(g, a, twz); });
         }
         if (g.ny > 1) {
             PassArgs<R> b;
             b.nf = nf;
             for (int f = 0; f < nf; ++f) {
-                b.in[f] = zi + (size_t)f * zsize;
+                b.in[f] = zi + (size_t)ysrc[f] * zsize;
                 b.out[f] = yi + (size_t)f * ysize;
-                b.op[f] = OP_ID;
+                b.op[f] = yops[f];
             }
             const double ybytes = nf * cb() * g.nkxc * g.nz * (double)(g.nkyc + g.ny);
             const bool yf = with_plan(g.ny, [&](auto Tc, auto Ec) {
@@ -886,6 +898,7 @@ public:
         XFastArgs<R> a;
         a.nin = nin;
         a.nout = nout;
+        a.dx_in_pass = 0;
         for (int f = 0; f < nin; ++f) a.in[f] = yi + (size_t)f * ysize;
         for (int f = 0; f < nout; ++f) a.out[f] = xo + (size_t)f * ysize;
         return a;
@@ -932,9 +945,10 @@ public:
         });
     }
 
-    void xb_launch(int nin, int nout, const PWB<R> &pw, int nreal)
+    void xb_launch(int nin, int nout, const PWB<R> &pw, int nreal, bool dx_in_pass)
     {
-        const XFastArgs<R> a = xargs(nin, nout);
+        XFastArgs<R> a = xargs(nin, nout);
+        a.dx_in_pass = dx_in_pass ? 1 : 0;
         const int nrows = g.ny * g.nz;
         with_plan(g.nx, [&](auto Tc, auto Ec) {
             constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value;
@@ -1062,17 +1076,57 @@ public:
                [&] { combine_a_kernel<R><<<combine_grid(), 256, 0, st>>>(g, ph, nm, c, ctrl, stage); });
     }
 
-    void phase_b(int stage, bool rhs_only)
+    // phase B's inverse transforms into YI buffers 0..nf-1; returns nf.
+    // dx_in_pass: the staged x pass takes d/dx itself, so the x and y
+    // derivatives of mu and of each Pi component share one z transform (k_x
+    // and k_y are constant along z) and each field is z-transformed twice,
+    // not three times.
+    int phase_b_inverse(bool &dx_in_pass)
     {
         const cplx<R> *src[MAXF];
         int ops[MAXF];
         int nf = 0;
-        for (int d = 0; d < nm; ++d) { src[nf] = MU; ops[nf++] = OP_IKX + d; }
-        if (ph.evolve)
-            for (int cp = 0; cp < 3; ++cp)
-                for (int d = 0; d < nm; ++d)
-                    for (int h = 0; h < 2; ++h) { src[nf] = P[2 * cp + h]; ops[nf++] = OP_IKX + d; }
-        inverse(nf, src, ops);
+        dx_in_pass = fast_x && staged_x && g.ny > 1 && has_plan(g.ny);
+        if (dx_in_pass) {
+            int nzf = 0, ysrc[MAXF], yops[MAXF];
+            auto field = [&](const cplx<R> *f) {
+                const int z0 = nzf;
+                src[nzf] = f; ops[nzf++] = OP_ID;
+                src[nzf] = f; ops[nzf++] = OP_IKZ;
+                return z0;
+            };
+            const int zmu = field(MU);
+            for (int d = 0; d < nm; ++d) {
+                ysrc[nf] = d == 2 ? zmu + 1 : zmu;
+                yops[nf++] = d == 1 ? OP_IKY : OP_ID;
+            }
+            if (ph.evolve) {
+                int zq[6];
+                for (int q = 0; q < 6; ++q) zq[q] = field(P[q]);
+                for (int cp = 0; cp < 3; ++cp)
+                    for (int d = 0; d < nm; ++d)
+                        for (int h = 0; h < 2; ++h) {
+                            const int z0 = zq[2 * cp + h];
+                            ysrc[nf] = d == 2 ? z0 + 1 : z0;
+                            yops[nf++] = d == 1 ? OP_IKY : OP_ID;
+                        }
+            }
+            inverse_shared(nzf, src, ops, nf, ysrc, yops);
+        } else {
+            for (int d = 0; d < nm; ++d) { src[nf] = MU; ops[nf++] = OP_IKX + d; }
+            if (ph.evolve)
+                for (int cp = 0; cp < 3; ++cp)
+                    for (int d = 0; d < nm; ++d)
+                        for (int h = 0; h < 2; ++h) { src[nf] = P[2 * cp + h]; ops[nf++] = OP_IKX + d; }
+            inverse(nf, src, ops);
+        }
+        return nf;
+    }
+
+    void phase_b(int stage, bool rhs_only)
+    {
+        bool dxp = false;
+        const int nf = phase_b_inverse(dxp);
         PWB<R> pw;
         pw.ph = ph;
         pw.nm = nm;
@@ -1094,7 +1148,7 @@ public:
             });
             launch("force_mean", 0.0, [&] { gauss_force_final_kernel<<<1, 32, 0, st>>>(spart, red_blocks, ctrl); });
         }
-        if (fast_x) xb_launch(nf, nout, pw, ph.evolve ? 1 + nm : 1);
+        if (fast_x) xb_launch(nf, nout, pw, ph.evolve ? 1 + nm : 1, dxp);
         else xpass(nf, nout, pw, xrb_b, "xpass_b", ph.evolve ? 1 + nm : 1);
         forward(nout, OB);
         CombineB<R> c;
@@ -1390,14 +1444,6 @@ public:
             }
         }
         // the phase-B pass sequence of stage 0
-        const cplx<R> *src[MAXF];
-        int ops[MAXF];
-        int nf = 0;
-        for (int d = 0; d < nm; ++d) { src[nf] = MU; ops[nf++] = OP_IKX + d; }
-        if (ph.evolve)
-            for (int cp = 0; cp < 3; ++cp)
-                for (int d = 0; d < nm; ++d)
-                    for (int h = 0; h < 2; ++h) { src[nf] = P[2 * cp + h]; ops[nf++] = OP_IKX + d; }
         const int nout = nm + (ph.evolve ? 6 : 0);
         PWB<R> pw;
         pw.ph = ph;
@@ -1422,8 +1468,9 @@ public:
             float best = 1e30f;
             for (int rep = 0; rep < 3; ++rep) {
                 cudaEventRecord(e0, st);
-                inverse(nf, src, ops);
-                if (fast_x) xb_launch(nf, nout, pw, ph.evolve ? 1 + nm : 1);
+                bool dxp = false;
+                const int nf = phase_b_inverse(dxp);
+                if (fast_x) xb_launch(nf, nout, pw, ph.evolve ? 1 + nm : 1, dxp);
                 else xpass(nf, nout, pw, xrb_b, "xpass_b", ph.evolve ? 1 + nm : 1);
                 forward(nout, OB);
                 cudaEventRecord(e1, st);
