@@ -495,9 +495,12 @@ __host__ __device__ __forceinline__ int pi_idx(int i, int j)
     return i == 0 ? (j == 1 ? 3 : 4) : 5;
 }
 
-template <typename R>
-__global__ void combine_a_kernel(Grid g, Phys ph, int nm, CombineA<R> c, Ctrl *ctrl, int stage)
+// NM: the number of momentum components (1, 2, 3) as a compile-time
+// constant, so that every small per-mode array below stays in registers
+template <typename R, int NM>
+__global__ void combine_a_kernel(Grid g, Phys ph, CombineA<R> c, Ctrl *ctrl, int stage)
 {
+    constexpr int nm = NM;
     const size_t total = (size_t)g.nkzc * g.nkyc * g.pkx;
     const int pending = ctrl->pending;
     const double phi = ctrl->pend_phi;
@@ -618,9 +621,10 @@ struct CombineB {
     cplx<R> *oN, *oM[3], *oP[6];     // rhs-only outputs (no update when set)
 };
 
-template <typename R>
-__global__ void combine_b_kernel(Grid g, Phys ph, int nm, CombineB<R> c, Ctrl *ctrl, int stage, int rhs_only)
+template <typename R, int NM>
+__global__ void combine_b_kernel(Grid g, Phys ph, CombineB<R> c, Ctrl *ctrl, int stage, int rhs_only)
 {
+    constexpr int nm = NM;
     const size_t total = (size_t)g.nkzc * g.nkyc * g.pkx;
     const StageScal s = ctrl->st[stage];
     const double dt = ctrl->dt;
@@ -725,9 +729,10 @@ struct CombineU {
     const cplx<R> *U[3];
 };
 
-template <typename R>
-__global__ void combine_u_kernel(Grid g, Phys ph, int nm, CombineU<R> c, Ctrl *ctrl)
+template <typename R, int NM>
+__global__ void combine_u_kernel(Grid g, Phys ph, CombineU<R> c, Ctrl *ctrl)
 {
+    constexpr int nm = NM;
     const size_t total = (size_t)g.nkzc * g.nkyc * g.pkx;
     const double phi = ctrl->pend_phi, ee = ctrl->pend_e;
     for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;

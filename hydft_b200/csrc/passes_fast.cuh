@@ -44,6 +44,19 @@ __host__ __device__ constexpr bool band_none(int e)
     return T * e > band_m<T, E>() && T * e + T - 1 < T * E - band_m<T, E>();
 }
 
+// k0 times the signed index of stride-layout element e (n = t + T e) of an
+// axis of length L, as kt + (T e or T e - L) k0 with kt = t k0: one fused
+// multiply-add, whose half BAND fixes at compile time (the same expression
+// either way, so both paths round alike)
+template <typename R, int T, int E, bool BAND>
+__device__ __forceinline__ R band_k(int e, int t, R k0, R kt)
+{
+    constexpr int L = T * E;
+    if (BAND && band_all_lo<T, E>(e)) return kt + R(T * e) * k0;
+    if (BAND && band_all_hi<T, E>(e)) return kt + R(T * e - L) * k0;
+    return kt + R(t + T * e <= L / 2 ? T * e : T * e - L) * k0;
+}
+
 template <typename R, int T, int E, bool BAND>
 __device__ __forceinline__ void load_band(cplx<R> (&v)[E], const cplx<R> *__restrict__ col, int rs, int t, int Mrt,
                                           int nc, bool valid)
@@ -125,6 +138,7 @@ __global__ void __launch_bounds__(TX * T * G) zinv_fast(Grid g, PassArgs<R> a, c
     for (int i = tid; i < 2 * L; i += blockDim.x) tw[i] = twz[i];
     const int my = valid ? signed_idx(kyc, g.My) : 0;
     const R kx = R(x * g.kx0), ky = R(my * g.ky0);
+    const R kz0 = R(g.kz0), kzt = R(t) * kz0;
     // kz runs over the compact band: element stride nkyc * pkx
     const int rs = g.nkyc * g.pkx;
     const size_t col = (size_t)kyc * g.pkx + x;
@@ -148,13 +162,13 @@ __global__ void __launch_bounds__(TX * T * G) zinv_fast(Grid g, PassArgs<R> a, c
     case OP_IKZ:
 #pragma unroll
         for (int e = 0; e < E; ++e)
-            if (!(BAND && band_none<T, E>(e))) v[e] = ik_times(R(fft_signed(t + T * e, L) * g.kz0), v[e]);
+            if (!(BAND && band_none<T, E>(e))) v[e] = ik_times(band_k<R, T, E, BAND>(e, t, kz0, kzt), v[e]);
         break;
     case OP_NK2:
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             if (BAND && band_none<T, E>(e)) continue;
-            const R kz = R(fft_signed(t + T * e, L) * g.kz0);
+            const R kz = band_k<R, T, E, BAND>(e, t, kz0, kzt);
             v[e] = R(-(kx * kx + ky * ky + kz * kz)) * v[e];
         }
         break;
@@ -182,9 +196,10 @@ __global__ void __launch_bounds__(TX * T * G) yinv_fast(Grid g, PassArgs<R> a, c
     // OP_IKY: the y derivative of a field whose z transform is shared with
     // other derivatives (k_y is constant along z); uniform over the block
     if (a.op[f] == OP_IKY) {
+        const R ky0 = R(g.ky0), kyt = R(t) * ky0;
 #pragma unroll
         for (int e = 0; e < E; ++e)
-            if (!(BAND && band_none<T, E>(e))) v[e] = ik_times(R(fft_signed(t + T * e, L) * g.ky0), v[e]);
+            if (!(BAND && band_none<T, E>(e))) v[e] = ik_times(band_k<R, T, E, BAND>(e, t, ky0, kyt), v[e]);
     }
     __syncthreads();
     stride_to_block<T, E, +1, R, BarBlock, TX>(v, t, xb + gi * (L + L / T) * TX + c, tw);
@@ -259,22 +274,24 @@ __device__ __forceinline__ void x_c2r_load(cplx<R> (&v)[E], const cplx<R> *__res
     constexpr int L = T * E;
     const int Mx = BAND ? band_m<T, E>() : Mrt;
     const cplx<R> zero = {R(0), R(0)};
-    auto get = [&](int kk, cplx<R> &va, cplx<R> &vb) {
+    const R kxt = R(t) * kx0;
+    // half-spectrum entries kk of a and b; kxk = kk kx0 for the derivative
+    auto get = [&](int kk, R kxk, cplx<R> &va, cplx<R> &vb) {
         va = ina[base + kk];
         vb = inb ? inb[base + kk] : zero;
-        if (dxa) va = ik_times(R(kk) * kx0, va);
-        if (dxb) vb = ik_times(R(kk) * kx0, vb);
+        if (dxa) va = ik_times(kxk, va);
+        if (dxb) vb = ik_times(kxk, vb);
     };
-    // k <= Mx: a_k + i b_k; k >= L - Mx: conj(a_{L-k}) + i conj(b_{L-k})
-    auto lo = [&](int k) {
+    // k = t + T e <= Mx: a_k + i b_k; k >= L - Mx: conj(a_{L-k}) + i conj(b_{L-k})
+    auto lo = [&](int k, int e) {
         cplx<R> va, vb;
-        get(k, va, vb);
+        get(k, kxt + R(T * e) * kx0, va, vb);
         if (k == 0) { va.y = R(0); vb.y = R(0); }
         return cplx<R>{va.x - vb.y, va.y + vb.x};
     };
-    auto hi = [&](int k) {
+    auto hi = [&](int k, int e) {
         cplx<R> va, vb;
-        get(L - k, va, vb);
+        get(L - k, R(L - T * e) * kx0 - kxt, va, vb);
         return cplx<R>{va.x + vb.y, -va.y + vb.x};
     };
 #pragma unroll
@@ -283,14 +300,14 @@ __device__ __forceinline__ void x_c2r_load(cplx<R> (&v)[E], const cplx<R> *__res
         if (BAND && band_none<T, E>(e)) {
             v[e] = cplx<R>{R(-0.0), R(-0.0)};
         } else if (BAND && band_all_lo<T, E>(e)) {
-            v[e] = rowok ? lo(k) : zero;
+            v[e] = rowok ? lo(k, e) : zero;
         } else if (BAND && band_all_hi<T, E>(e)) {
-            v[e] = rowok ? hi(k) : zero;
+            v[e] = rowok ? hi(k, e) : zero;
         } else {
             cplx<R> Z = zero;
             if (rowok) {
-                if (k <= Mx) Z = lo(k);
-                else if (k >= L - Mx) Z = hi(k);
+                if (k <= Mx) Z = lo(k, e);
+                else if (k >= L - Mx) Z = hi(k, e);
             }
             v[e] = Z;
         }

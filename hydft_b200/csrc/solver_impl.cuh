@@ -1028,6 +1028,16 @@ public:
         launch(name, bytes, [&] { xpass_kernel<R, PW><<<(nrows + rb - 1) / rb, 256, sm, st>>>(g, a, twx, pw, rb); });
     }
 
+    // f(integral_constant<int, nm>): the momentum component count as a
+    // compile-time constant
+    template <class F>
+    void with_nm(F &&f) const
+    {
+        if (nm == 3) f(std::integral_constant<int, 3>{});
+        else if (nm == 2) f(std::integral_constant<int, 2>{});
+        else f(std::integral_constant<int, 1>{});
+    }
+
     int combine_grid() const
     {
         return (int)std::min<size_t>((csize + 255) / 256, 148 * 16);
@@ -1073,7 +1083,7 @@ public:
         const double ncomp = (double)g.nkxc * g.nkyc * g.nkzc;
         const int nrw = 2 + nm + nm * (nm + 1) / 2 + 1 + nm + (ph.evolve ? 24 : 0);
         launch("combine_a", ncomp * (cb() * nrw + sizeof(R)),
-               [&] { combine_a_kernel<R><<<combine_grid(), 256, 0, st>>>(g, ph, nm, c, ctrl, stage); });
+               [&] { with_nm([&](auto n) { combine_a_kernel<R, decltype(n)::value><<<combine_grid(), 256, 0, st>>>(g, ph, c, ctrl, stage); }); });
     }
 
     // phase B's inverse transforms into YI buffers 0..nf-1; returns nf.
@@ -1165,7 +1175,9 @@ public:
         const double ncomp = (double)g.nkxc * g.nkyc * g.nkzc;
         const int nrw = 2 + 5 * nm + 2 + (ph.evolve ? 30 : 0);
         launch("combine_b", ncomp * cb() * nrw, [&] {
-            combine_b_kernel<R><<<combine_grid(), 256, 0, st>>>(g, ph, nm, c, ctrl, stage, rhs_only ? 1 : 0);
+            with_nm([&](auto n) {
+                combine_b_kernel<R, decltype(n)::value><<<combine_grid(), 256, 0, st>>>(g, ph, c, ctrl, stage, rhs_only ? 1 : 0);
+            });
         });
     }
 
@@ -1225,7 +1237,7 @@ public:
         for (int d = 0; d < 3; ++d) c.U[d] = OA[std::min(d, nm - 1)];
         const double ncomp = (double)g.nkxc * g.nkyc * g.nkzc;
         launch("combine_u", ncomp * cb() * (nm + 18),
-               [&] { combine_u_kernel<R><<<combine_grid(), 256, 0, st>>>(g, ph, nm, c, ctrl); });
+               [&] { with_nm([&](auto n) { combine_u_kernel<R, decltype(n)::value><<<combine_grid(), 256, 0, st>>>(g, ph, c, ctrl); }); });
         cudaMemsetAsync(&ctrl->pending, 0, sizeof(int), st);
     }
 
