@@ -265,8 +265,11 @@ __host__ __device__ constexpr int xrow_stride() { return (T * E + E + 15) / 16 *
 //
 // dxa / dxb: the input is differentiated along x on the way in (a_k becomes
 // i k kx0 a_k), for fields whose z and y transforms are shared with their
-// other derivatives.
-template <typename R, int T, int E, bool BAND = false>
+// other derivatives.  BM: inb is null (0), not null (1) or tested (2).
+// Loads from rows staged in shared memory pass rowok = true: every staged
+// row slot exists (unused ones hold stale data whose results are not
+// stored).
+template <typename R, int T, int E, bool BAND = false, int BM = 2>
 __device__ __forceinline__ void x_c2r_load(cplx<R> (&v)[E], const cplx<R> *__restrict__ ina,
                                            const cplx<R> *__restrict__ inb, size_t base, bool rowok, int t, int Mrt,
                                            bool dxa = false, bool dxb = false, R kx0 = R(0))
@@ -278,7 +281,7 @@ __device__ __forceinline__ void x_c2r_load(cplx<R> (&v)[E], const cplx<R> *__res
     // half-spectrum entries kk of a and b; kxk = kk kx0 for the derivative
     auto get = [&](int kk, R kxk, cplx<R> &va, cplx<R> &vb) {
         va = ina[base + kk];
-        vb = inb ? inb[base + kk] : zero;
+        vb = (BM == 1 || (BM == 2 && inb)) ? inb[base + kk] : zero;
         if (dxa) va = ik_times(kxk, va);
         if (dxb) vb = ik_times(kxk, vb);
     };
@@ -324,27 +327,40 @@ __device__ __forceinline__ void x_c2r_pair(cplx<R> (&v)[E], const cplx<R> *__res
 }
 
 // r2c of z = a + i b given in block layout; writes the half spectra of a
-// and b for kx <= Mx (outb may be null)
-template <typename R, int T, int E, bool BAND = false>
+// and b for kx <= Mx (outb null (BM 0), not null (1) or tested (2)).  UNR
+// with BAND: the output loop is unrolled over the compile-time band
+// classification (no divergent trip count; more registers live)
+template <typename R, int T, int E, bool BAND = false, int BM = 2, bool UNR = false>
 __device__ __forceinline__ void x_r2c_pair(cplx<R> (&v)[E], cplx<R> *__restrict__ outa, cplx<R> *__restrict__ outb,
                                            int row, bool rowok, int t, const Grid &g, cplx<R> *xrow,
                                            const cplx<R> *tw)
 {
     constexpr int L = T * E;
     block_to_stride<T, E, -1, R, BarWarp, 1>(v, t, xrow, tw);
+    // element t + T m; with BAND the ones outside the band for every t are
+    // never read below, so neither they nor their last butterflies are made
 #pragma unroll
-    for (int m = 0; m < E; ++m) xrow[t + m * (T + 1)] = v[m];   // element t + T m
+    for (int m = 0; m < E; ++m)
+        if (!(BAND && band_none<T, E>(m))) xrow[t + m * (T + 1)] = v[m];
     __syncwarp();
     const size_t base = (size_t)row * g.pkx;
     auto put = [&](int k) {
         const cplx<R> zk = xrow[xidx<T>(k)];
         const cplx<R> zm = conj(xrow[xidx<T>(k == 0 ? 0 : L - k)]);
         outa[base + k] = R(0.5) * (zk + zm);
-        if (outb) outb[base + k] = mul_i<-1>(R(0.5) * (zk - zm));
+        if (BM == 1 || (BM == 2 && outb)) outb[base + k] = mul_i<-1>(R(0.5) * (zk - zm));
     };
     if (rowok) {
-        const int Mx = BAND ? band_m<T, E>() : g.Mx;
-        for (int k = t; k <= Mx; k += T) put(k);
+        if (BAND && UNR) {
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                if (band_all_lo<T, E>(e)) put(t + T * e);
+                else if (T * e <= band_m<T, E>() && t + T * e <= band_m<T, E>()) put(t + T * e);
+            }
+        } else {
+            const int Mx = BAND ? band_m<T, E>() : g.Mx;
+            for (int k = t; k <= Mx; k += T) put(k);
+        }
     }
     __syncwarp();
 }
@@ -614,7 +630,8 @@ __host__ __device__ constexpr int xstaged_minb() { return sizeof(R) == 4 && E <=
 // Phase A without Fermi-Dirac terms (ideal / Hartree / RY ions and the u-only
 // relaxation finish): the four inputs dn, m_0..m_2 stay in registers as two
 // pairs, so no per-thread shared-memory slots are needed and two 256-thread
-// blocks fit on an SM.  The output pairs are ordered so that dn is consumed
+// blocks fit on an SM.  The block's spectral input rows are copied into
+// shared memory by cp.async first.  The output pairs are ordered so that dn is consumed
 // first: (mu_local, u_0), (u_1, u_2), (m0u0, m0u1), (m0u2, m1u1), (m1u2, m2u2);
 // UONLY: (u_0, u_1), (u_2, -).  Outputs go to the same fields as xa_fast's.
 template <typename R, int T, int E, bool UONLY, bool BAND>
@@ -623,22 +640,31 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xa_regs(Grid g, XFa
     constexpr int L = T * E;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
-    cplx<R> *xbuf = tw + 2 * L;
-    const int nt = blockDim.x, rb = nt / T;
+    const int nt = blockDim.x, rb = nt / T, pk = g.pkx;
+    cplx<R> *sb = tw + 2 * L;                      // [4][rb][pkx] the staged inputs
+    cplx<R> *xbuf = sb + 4 * (size_t)rb * pk;
     const int tid = threadIdx.x, t = tid % T, rr = tid / T;
-    const int row = blockIdx.x * rb + rr;
+    const int row0 = blockIdx.x * rb, row = row0 + rr;
     const bool rowok = row < g.ny * g.nz;
+    const int vrows = max(0, min(rb, g.ny * g.nz - row0));
     cplx<R> *xrow = xbuf + rr * xrow_stride<T, E>();
-    {
-        const int row0 = blockIdx.x * rb;
-        XPrefetch<R> pf(a, g, row0, max(0, min(rb, g.ny * g.nz - row0)), tid == 0);
-        pf.upto(3);
+    // the block's rows of all four inputs on their way at once, one commit
+    // group per pair: pair 1 lands while pair 0 is transformed
+    for (int f = 0; f < 4; ++f) {
+        stage_rows(sb + (size_t)f * rb * pk, a.in[f], row0, vrows, pk, tid, nt);
+        if (f & 1) cp_async_commit();
     }
     for (int i = tid; i < 2 * L; i += nt) tw[i] = twx[i];
-    __syncthreads();
     cplx<R> p0[E], p1[E];   // (dn, m_0), (m_1, m_2)
-    x_c2r_pair<R, T, E, BAND>(p0, a.in[0], a.in[1], row, rowok, t, g, xrow, tw);
-    x_c2r_pair<R, T, E, BAND>(p1, a.in[2], a.in[3], row, rowok, t, g, xrow, tw);
+    const size_t sbase = (size_t)rr * pk;
+    cp_async_wait_one();
+    __syncthreads();
+    x_c2r_load<R, T, E, BAND, 1>(p0, sb, sb + (size_t)rb * pk, sbase, true, t, g.Mx);
+    stride_to_block<T, E, +1, R, BarWarp, 1>(p0, t, xrow, tw);
+    cp_async_wait_all();
+    __syncthreads();
+    x_c2r_load<R, T, E, BAND, 1>(p1, sb + 2 * (size_t)rb * pk, sb + 3 * (size_t)rb * pk, sbase, true, t, g.Mx);
+    stride_to_block<T, E, +1, R, BarWarp, 1>(p1, t, xrow, tw);
     const double nref64 = *pw.nmean;
     const R nref = R(nref64);
     const R inv_nref = R(1) / nref, inv_beta = R(pw.ph.inv_beta), mass = R(pw.ph.mass);
@@ -672,33 +698,33 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xa_regs(Grid g, XFa
     }
     if (!UONLY) {
         // outputs: 0..2 u_d, 3..8 fluxes (00, 01, 02, 11, 12, 22), 9 mu
-        x_r2c_pair<R, T, E, BAND>(v, a.out[9], a.out[0], row, rowok, t, g, xrow, tw);
+        x_r2c_pair<R, T, E, BAND, 1>(v, a.out[9], a.out[0], row, rowok, t, g, xrow, tw);
 #pragma unroll
         for (int r = 0; r < E; ++r) v[r] = cplx<R>{p1[r].x * p0[r].x, p1[r].y * p0[r].x};
-        x_r2c_pair<R, T, E, BAND>(v, a.out[1], a.out[2], row, rowok, t, g, xrow, tw);
+        x_r2c_pair<R, T, E, BAND, 1>(v, a.out[1], a.out[2], row, rowok, t, g, xrow, tw);
 #pragma unroll
         for (int r = 0; r < E; ++r) {
             const R u0 = p0[r].y * p0[r].x;
             v[r] = cplx<R>{p0[r].y * u0, p0[r].y * (p1[r].x * p0[r].x)};
         }
-        x_r2c_pair<R, T, E, BAND>(v, a.out[3], a.out[4], row, rowok, t, g, xrow, tw);
+        x_r2c_pair<R, T, E, BAND, 1>(v, a.out[3], a.out[4], row, rowok, t, g, xrow, tw);
 #pragma unroll
         for (int r = 0; r < E; ++r) {
             const R u1 = p1[r].x * p0[r].x, u2 = p1[r].y * p0[r].x;
             v[r] = cplx<R>{p0[r].y * u2, p1[r].x * u1};
         }
-        x_r2c_pair<R, T, E, BAND>(v, a.out[5], a.out[6], row, rowok, t, g, xrow, tw);
+        x_r2c_pair<R, T, E, BAND, 1>(v, a.out[5], a.out[6], row, rowok, t, g, xrow, tw);
 #pragma unroll
         for (int r = 0; r < E; ++r) {
             const R u2 = p1[r].y * p0[r].x;
             v[r] = cplx<R>{p1[r].x * u2, p1[r].y * u2};
         }
-        x_r2c_pair<R, T, E, BAND>(v, a.out[7], a.out[8], row, rowok, t, g, xrow, tw);
+        x_r2c_pair<R, T, E, BAND, 1>(v, a.out[7], a.out[8], row, rowok, t, g, xrow, tw);
     } else {
-        x_r2c_pair<R, T, E, BAND>(v, a.out[0], a.out[1], row, rowok, t, g, xrow, tw);
+        x_r2c_pair<R, T, E, BAND, 1>(v, a.out[0], a.out[1], row, rowok, t, g, xrow, tw);
 #pragma unroll
         for (int r = 0; r < E; ++r) v[r] = cplx<R>{p1[r].y * p0[r].x, R(0)};
-        x_r2c_pair<R, T, E, BAND>(v, a.out[2], nullptr, row, rowok, t, g, xrow, tw);
+        x_r2c_pair<R, T, E, BAND, 0>(v, a.out[2], nullptr, row, rowok, t, g, xrow, tw);
     }
 }
 
@@ -772,13 +798,16 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xb_rows(Grid g, XFa
     // the staged pair p into registers, then pair p + 1 on its way
     const R kx0 = R(g.kx0);
     const bool dxs = a.dx_in_pass != 0;
-    auto load = [&](int p, cplx<R> (&v)[E], bool dxa, bool dxb) {
+    using B0 = std::integral_constant<int, 0>;   // a pair without its second field
+    using B1 = std::integral_constant<int, 1>;
+    auto load = [&](int p, cplx<R> (&v)[E], bool dxa, bool dxb, auto bm) {
+        constexpr int BM = decltype(bm)::value;
         int fa, fb;
         fields(p, fa, fb);
         cp_async_wait_all();
         __syncthreads();
-        x_c2r_load<R, T, E, BAND>(v, sb, fb >= 0 ? sb + (size_t)rb * pk : nullptr, (size_t)rr * pk, rowok, t, g.Mx,
-                                  dxa, dxb, kx0);
+        x_c2r_load<R, T, E, BAND, BM>(v, sb, BM ? sb + (size_t)rb * pk : nullptr, (size_t)rr * pk, true, t, g.Mx,
+                                      dxa, dxb, kx0);
         __syncthreads();
         stage(p + 1);
         pf.upto((fb >= 0 ? fb : fa) + 2 + AHEAD);
@@ -791,7 +820,8 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xb_rows(Grid g, XFa
     for (int q = 0; 2 * q < NM; ++q) {
         const int i0 = 2 * q, i1 = 2 * q + 1;
         cplx<R> v[E];
-        load(q, v, dxs && q == 0, false);   // d/dx of mu
+        if (i1 < NM) load(q, v, dxs && q == 0, false, B1{});   // d/dx of mu
+        else load(q, v, false, false, B0{});
         stride_to_block<T, E, +1, R, BarWarp, 1>(v, t, xrow, tw);
 #pragma unroll
         for (int r = 0; r < E; ++r) {
@@ -812,7 +842,8 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xb_rows(Grid g, XFa
             }
             v[r] = cplx<R>{n * (v[r].x - f0), n * (v[r].y - f1)};
         }
-        x_r2c_pair<R, T, E, BAND>(v, a.out[i0], i1 < NM ? a.out[i1] : nullptr, row, rowok, t, g, xrow, tw);
+        if (i1 < NM) x_r2c_pair<R, T, E, BAND, 1, true>(v, a.out[i0], a.out[i1], row, rowok, t, g, xrow, tw);
+        else x_r2c_pair<R, T, E, BAND, 0, true>(v, a.out[i0], nullptr, row, rowok, t, g, xrow, tw);
     }
     if (EVOLVE) {
         // -u.grad Pi for component pairs (0,1), (2,3), (4,5)
@@ -824,13 +855,14 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xb_rows(Grid g, XFa
 #pragma unroll
             for (int d = 0; d < NM; ++d) {
                 cplx<R> v[E];
-                load(2 + cp * NM + d, v, dxs && d == 0, dxs && d == 0);   // d/dx of Pi
+                load(2 + cp * NM + d, v, dxs && d == 0, dxs && d == 0, B1{});   // d/dx of Pi
                 stride_to_block<T, E, +1, R, BarWarp, 1>(v, t, xrow, tw);
                 const R *urow = rs + ((size_t)d * rb + rr) * RS;
 #pragma unroll
                 for (int r = 0; r < E; ++r) acc[r] = acc[r] - urow[block_pos<T, E>(t, r)] * v[r];
             }
-            x_r2c_pair<R, T, E, BAND>(acc, a.out[NM + 2 * cp], a.out[NM + 2 * cp + 1], row, rowok, t, g, xrow, tw);
+            x_r2c_pair<R, T, E, BAND, 1, true>(acc, a.out[NM + 2 * cp], a.out[NM + 2 * cp + 1], row, rowok, t, g,
+                                               xrow, tw);
         }
     }
 }

@@ -924,8 +924,15 @@ public:
                 launch(name, xbytes(nin, nout, nreal), [&] { k<<<(nrows + rb - 1) / rb, nt, sm, st>>>(g, a, tpx, pw); });
             };
             auto go_regs = [&](auto k) {
-                const int nt = std::min(256, x_ntmax) / T * T;
-                const size_t sm = xstaged_smem<R, T, E>(nt, g.pkx, 0, 0);
+                int nt = std::min(256, x_ntmax) / T * T;
+                size_t sm = xstaged_smem<R, T, E>(nt, g.pkx, 4, 0);
+                // the blocks per SM the kernel is compiled for must fit: 228 KB
+                // of shared memory per SM, 1 KB reserved per block
+                const size_t cap = xstaged_minb<R, E>() == 2 ? 115712 : (size_t)smem_optin;
+                while (sm > cap && nt > T) {
+                    nt /= 2;
+                    sm = xstaged_smem<R, T, E>(nt, g.pkx, 4, 0);
+                }
                 set_smem(k, sm);
                 const int rb = nt / T;
                 launch(name, xbytes(nin, nout, nreal), [&] { k<<<(nrows + rb - 1) / rb, nt, sm, st>>>(g, a, tpx, pw); });
