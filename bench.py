@@ -510,9 +510,12 @@ def main():
     cells = float(n) ** 3
     value = cells * args.steps * world / (ms_max * 1e-3)
     ms_step = ms_max / args.steps
+    # the autotuned tile shapes the timed steps ran with
+    tiles = {"yz_columns": int(m32.scalar("yz_tile")), "yz_threads": int(m32.scalar("yz_threads")),
+             "x_threads": int(m32.scalar("x_threads"))}
     if args.quick:
         if rank == 0:
-            print(json.dumps({"quick": True, "grid": n, "precision": args.precision, "value": value,
+            print(json.dumps({"quick": True, "grid": n, "precision": args.precision, "value": value, "tiles": tiles,
                               "ms_per_step": ms_step, "gpu_launches": int(gpu_launches)}), flush=True)
         m32.close()
         if dist is not None:
@@ -635,7 +638,7 @@ def main():
                            "gamma": 50.0, "kappa": 2.0, "closure": "maxwell", "tau_model": "ichimaru",
                            "transport": "yukawa_fit", "dt": dt, "precision": "fp32 fields, fp64 sums",
                            "parallelism": "replicas" if world > 1 else "single",
-                           "l2": "inputs larger than L2 (working set ~GBs)"},
+                           "l2": "inputs larger than L2 (working set ~GBs)", "tiles": tiles},
                 "roofline": roof,
                 "step_roofline": {"bytes_per_cell_step": STEP_BYTES_FP32,
                                   "achieved_GBps": STEP_BYTES_FP32 * value / world / 1e9,

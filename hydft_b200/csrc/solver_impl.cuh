@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <array>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -427,6 +428,7 @@ public:
     bool band_x = false, band_y = false, band_z = false;
     // tile shapes picked by tune(): kx columns per y/z block, threads per x block
     int yz_tx = sizeof(R) == 4 ? 16 : 8;
+    int yz_nt = sizeof(R) == 4 ? 256 : 128;
     int x_ntmax = 256;
     bool tuned = false;
     size_t alloc_bytes = 0;      // device memory allocated by this solver
@@ -734,12 +736,26 @@ public:
     // YI buffers 0..nf-1
     static constexpr int YZ_TX = sizeof(R) == 4 ? 16 : 8;
 
-    // the y/z passes' kx columns per block (8 or 16) as a compile-time constant
+    // the y/z passes' block shape as compile-time constants: kx columns per
+    // block (8 or 16) and threads per block (YZ_NT, or 2 YZ_NT, which the
+    // 256-point plan alone uses: a block then also spans two rows of the
+    // other axis, or 32 columns)
     template <class F>
-    void with_tx(F &&f) const
+    void with_yz(F &&f) const
     {
-        if (yz_tx == 8) f(std::integral_constant<int, 8>{});
-        else f(std::integral_constant<int, 16>{});
+        auto nt = [&](auto TXc) {
+            if (yz_nt == 2 * YZ_NT) f(TXc, std::integral_constant<int, 2 * YZ_NT>{});
+            else f(TXc, std::integral_constant<int, YZ_NT>{});
+        };
+        if (yz_tx == 8) nt(std::integral_constant<int, 8>{});
+        else nt(std::integral_constant<int, 16>{});
+    }
+    // rows of the other axis per y/z block for T threads per column
+    template <int T, int TX, int NTR>
+    static constexpr int yz_rows()
+    {
+        constexpr int NT = T == 16 ? NTR : YZ_NT;
+        return NT / (TX * T) > 0 ? NT / (TX * T) : 1;
     }
     static constexpr int YZ_NT = sizeof(R) == 4 ? 256 : 128;
 
@@ -775,9 +791,9 @@ public:
         const double zbytes = nzf * cb() * g.nkxc * g.nkyc * (double)(g.nkzc + g.nz);
         const bool zf = with_plan(g.nz, [&](auto Tc, auto Ec) {
             constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value;
-            with_tx([&](auto TXc) {
+            with_yz([&](auto TXc, auto NTc) {
             constexpr int TX = decltype(TXc)::value;
-            constexpr int G = YZ_NT / (TX * T) > 0 ? YZ_NT / (TX * T) : 1;
+            constexpr int G = yz_rows<T, TX, decltype(NTc)::value>();
             const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
             auto k = band_z ? zinv_fast<R, T, E, TX, G, true> : zinv_fast<R, T, E, TX, G, false>;
             set_smem(k, sm);
@@ -801,9 +817,9 @@ public:
             const double ybytes = nf * cb() * g.nkxc * g.nz * (double)(g.nkyc + g.ny);
             const bool yf = with_plan(g.ny, [&](auto Tc, auto Ec) {
                 constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value;
-                with_tx([&](auto TXc) {
+                with_yz([&](auto TXc, auto NTc) {
                 constexpr int TX = decltype(TXc)::value;
-                constexpr int G = YZ_NT / (TX * T) > 0 ? YZ_NT / (TX * T) : 1;
+                constexpr int G = yz_rows<T, TX, decltype(NTc)::value>();
                 const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
                 auto k = band_y ? yinv_fast<R, T, E, TX, G, true> : yinv_fast<R, T, E, TX, G, false>;
                 set_smem(k, sm);
@@ -835,9 +851,9 @@ public:
             const double ybytes = nf * cb() * g.nkxc * g.nz * (double)(g.nkyc + g.ny);
             const bool yf = with_plan(g.ny, [&](auto Tc, auto Ec) {
                 constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value;
-                with_tx([&](auto TXc) {
+                with_yz([&](auto TXc, auto NTc) {
                 constexpr int TX = decltype(TXc)::value;
-                constexpr int G = YZ_NT / (TX * T) > 0 ? YZ_NT / (TX * T) : 1;
+                constexpr int G = yz_rows<T, TX, decltype(NTc)::value>();
                 const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
                 auto k = band_y ? yfwd_fast<R, T, E, TX, G, true> : yfwd_fast<R, T, E, TX, G, false>;
                 set_smem(k, sm);
@@ -862,9 +878,9 @@ public:
         const double zbytes = nf * cb() * g.nkxc * g.nkyc * (double)(g.nkzc + g.nz);
         const bool zf = with_plan(g.nz, [&](auto Tc, auto Ec) {
             constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value;
-            with_tx([&](auto TXc) {
+            with_yz([&](auto TXc, auto NTc) {
             constexpr int TX = decltype(TXc)::value;
-            constexpr int G = YZ_NT / (TX * T) > 0 ? YZ_NT / (TX * T) : 1;
+            constexpr int G = yz_rows<T, TX, decltype(NTc)::value>();
             const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
             auto k = band_z ? zfwd_fast<R, T, E, TX, G, true> : zfwd_fast<R, T, E, TX, G, false>;
             set_smem(k, sm);
@@ -1319,10 +1335,11 @@ public:
 
     int prepare() override { return tune(); }
 
-    void tiles(int *yz, int *xnt) const override
+    void tiles(int *yz, int *xnt, int *yznt) const override
     {
         *yz = yz_tx;
         *xnt = x_ntmax;
+        *yznt = yz_nt;
     }
 
     int band_axes() const override { return (band_x ? 1 : 0) | (band_y ? 2 : 0) | (band_z ? 4 : 0); }
@@ -1427,9 +1444,10 @@ public:
             return std::tie(nx, ny, nz, bytes, nm, evolve, ext) < std::tie(o.nx, o.ny, o.nz, o.bytes, o.nm, o.evolve, o.ext);
         }
     };
-    static std::map<TuneKey, std::pair<int, int>> &tune_cache()
+    // cached shape: {kx columns per y/z block, threads per y/z block, threads per x block}
+    static std::map<TuneKey, std::array<int, 3>> &tune_cache()
     {
-        static std::map<TuneKey, std::pair<int, int>> m;
+        static std::map<TuneKey, std::array<int, 3>> m;
         return m;
     }
     static std::mutex &tune_mutex()
@@ -1444,11 +1462,14 @@ public:
         tuned = true;
         const char *ev = std::getenv("HYDFT_TUNE");
         if (ev && std::string(ev) == "0") return 0;
-        // fixed shapes on request (HYDFT_YZ_TILE = 8 | 16, HYDFT_X_THREADS = 128 | 256)
+        // fixed shapes on request (HYDFT_YZ_TILE = 8 | 16, HYDFT_YZ_THREADS =
+        // YZ_NT | 2 YZ_NT, HYDFT_X_THREADS = 128 | 256)
         const char *fy = std::getenv("HYDFT_YZ_TILE"), *fx = std::getenv("HYDFT_X_THREADS");
-        if ((fy && *fy) || (fx && *fx)) {
+        const char *fn = std::getenv("HYDFT_YZ_THREADS");
+        if ((fy && *fy) || (fx && *fx) || (fn && *fn)) {
             if (fy && (std::string(fy) == "8" || std::string(fy) == "16")) yz_tx = std::atoi(fy);
             if (fx && (std::string(fx) == "128" || std::string(fx) == "256")) x_ntmax = std::atoi(fx);
+            if (fn && (std::atoi(fn) == YZ_NT || std::atoi(fn) == 2 * YZ_NT)) yz_nt = std::atoi(fn);
             return 0;
         }
         if (!(has_plan(g.ny) || has_plan(g.nz))) return 0;
@@ -1457,8 +1478,9 @@ public:
             std::lock_guard<std::mutex> lk(tune_mutex());
             auto it = tune_cache().find(key);
             if (it != tune_cache().end()) {
-                yz_tx = it->second.first;
-                x_ntmax = it->second.second;
+                yz_tx = it->second[0];
+                yz_nt = it->second[1];
+                x_ntmax = it->second[2];
                 return 0;
             }
         }
@@ -1481,8 +1503,9 @@ public:
         cudaEvent_t e0, e1;
         CK(cudaEventCreate(&e0));
         CK(cudaEventCreate(&e1));
-        auto time_it = [&](int tx, int ntmax) -> float {
+        auto time_it = [&](int tx, int ynt, int ntmax) -> float {
             yz_tx = tx;
+            yz_nt = ynt;
             x_ntmax = ntmax;
             float best = 1e30f;
             for (int rep = 0; rep < 3; ++rep) {
@@ -1502,22 +1525,28 @@ public:
         };
         const int txs[2] = {8, 16};
         const int nts[2] = {128, 256};
+        const int ynts[2] = {YZ_NT, 2 * YZ_NT};
+        // the wide y/z blocks exist for the 256-point plan only
+        const bool wide = g.ny == 256 || g.nz == 256;
         float best = 1e30f;
-        int btx = yz_tx, bnt = x_ntmax;
+        int btx = yz_tx, bynt = yz_nt, bnt = x_ntmax;
         for (int tx : txs)
-            for (int nt : nts) {
-                if (!fast_x && nt != 256) continue;
-                const float ms = time_it(tx, nt);
-                if (ms < best) { best = ms; btx = tx; bnt = nt; }
-            }
+            for (int ynt : ynts)
+                for (int nt : nts) {
+                    if (!fast_x && nt != 256) continue;
+                    if (!wide && ynt != YZ_NT) continue;
+                    const float ms = time_it(tx, ynt, nt);
+                    if (ms < best) { best = ms; btx = tx; bynt = ynt; bnt = nt; }
+                }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         launches = launches0;
         yz_tx = btx;
+        yz_nt = bynt;
         x_ntmax = bnt;
         CK(cudaGetLastError());
         std::lock_guard<std::mutex> lk(tune_mutex());
-        tune_cache()[key] = {btx, bnt};
+        tune_cache()[key] = {btx, bynt, bnt};
         return 0;
     }
 

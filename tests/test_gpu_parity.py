@@ -343,3 +343,26 @@ def test_band_classified_passes_match_runtime_band_test(hg, monkeypatch, prec):
     m = hg.Model(hg.default_params(**dict(kw, dealias=False)))
     assert m.scalar("band_axes") == 0
     m.close()
+
+
+@pytest.mark.parametrize("prec,base", [("fp32", 256), ("fp64", 128)])
+def test_wide_yz_blocks_give_identical_results(hg, monkeypatch, prec, base):
+    """On 256-point y and z axes the autotuner also tries y/z blocks of twice
+    the threads (two rows of the other axis, or 32 kx columns, per block);
+    they give the same fields to the bit as the narrow blocks."""
+    kw = dict(ION, nx=32, ny=256, nz=256, lx=16.0, ly=128.0, lz=128.0, closure="maxwell", tau_model="constant",
+              tau=1.5, dt=0.01, gpu_precision=prec)
+    out = []
+    for tile, nt in (("16", base), ("16", 2 * base), ("8", 2 * base)):
+        monkeypatch.setenv("HYDFT_YZ_TILE", tile)
+        monkeypatch.setenv("HYDFT_YZ_THREADS", str(nt))
+        m = hg.Model(hg.default_params(**kw))
+        n, mom, pi = seeded_state(m)
+        m.set_state(n, mom, pi)
+        m.advance(2)
+        assert m.scalar("yz_tile") == int(tile) and m.scalar("yz_threads") == nt
+        out.append(m.get_state())
+        m.close()
+    for other in out[1:]:
+        for x, y in zip(out[0], other):
+            assert np.array_equal(x, y)
