@@ -511,7 +511,8 @@ def main():
     value = cells * args.steps * world / (ms_max * 1e-3)
     ms_step = ms_max / args.steps
     # the autotuned tile shapes the timed steps ran with
-    tiles = {"yz_columns": int(m32.scalar("yz_tile")), "yz_threads": int(m32.scalar("yz_threads")),
+    tiles = {"yz_inverse": [int(m32.scalar("yz_tile")), int(m32.scalar("yz_threads"))],
+             "yz_forward": [int(m32.scalar("yz_tile_fwd")), int(m32.scalar("yz_threads_fwd"))],
              "x_threads": int(m32.scalar("x_threads"))}
     if args.quick:
         if rank == 0:

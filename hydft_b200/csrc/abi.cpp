@@ -324,10 +324,12 @@ int hydft_gpu_get_scalar(const hydft_gpu *h, const char *name, double *v)
     else if (k == "evolve") *v = m.evolve ? 1.0 : 0.0;
     else if (k == "precision") *v = m.precision;
     else if (k == "device_bytes") *v = (double)h->s->device_bytes();
-    else if (k == "yz_tile" || k == "x_threads" || k == "yz_threads") {
-        int yz = 0, xn = 0, yn = 0;
-        h->s->tiles(&yz, &xn, &yn);
-        *v = k == "yz_tile" ? yz : (k == "x_threads" ? xn : yn);
+    else if (k == "yz_tile" || k == "yz_threads" || k == "yz_tile_fwd" || k == "yz_threads_fwd" ||
+             k == "x_threads") {
+        int t[5] = {0, 0, 0, 0, 0};
+        h->s->tiles(t);
+        const int i = k == "yz_tile" ? 0 : k == "yz_threads" ? 1 : k == "yz_tile_fwd" ? 2 : k == "yz_threads_fwd" ? 3 : 4;
+        *v = t[i];
     }
     else if (k == "band_axes") *v = h->s->band_axes();
     else if (k == "ext_omega") *v = m.ext_omega;

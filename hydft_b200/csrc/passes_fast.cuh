@@ -669,6 +669,10 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xa_regs(Grid g, XFa
     const R nref = R(nref64);
     const R inv_nref = R(1) / nref, inv_beta = R(pw.ph.inv_beta), mass = R(pw.ph.mass);
     const size_t rowbase = (size_t)row * g.nx;
+    // occurrences of the ideal term (the only local term this kernel has) in
+    // the term list, counted once rather than per element
+    int nid = 0;
+    for (int tt = 0; tt < pw.ph.nterms_local; ++tt) nid += pw.ph.term_order[tt] == 1;
     // mu_local (ideal terms in the given order) and 1/(m n); p0[r].x becomes 1/(m n)
     cplx<R> v[E];
 #pragma unroll
@@ -688,8 +692,11 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xa_regs(Grid g, XFa
         }
         if (!UONLY) {
             R mu = R(0);
-            for (int tt = 0; tt < pw.ph.nterms_local; ++tt)
-                if (pw.ph.term_order[tt] == 1) mu += log1p(dn * inv_nref) * inv_beta;
+            if (nid > 0) {
+                const R l = log1p(dn * inv_nref) * inv_beta;
+                mu += l;
+                for (int c = 1; c < nid; ++c) mu += l;
+            }
             v[r] = cplx<R>{mu, p0[r].y * inv_mn};
         } else {
             v[r] = cplx<R>{p0[r].y * inv_mn, p1[r].x * inv_mn};

@@ -79,9 +79,9 @@ public:
     // picks the tile shapes (autotuner) if not done yet; must precede a
     // capture of enqueue_steps
     virtual int prepare() = 0;
-    // tile shapes in use: kx columns per y/z block, threads per x block,
-    // threads per y/z block
-    virtual void tiles(int *yz, int *xnt, int *yznt) const = 0;
+    // tile shapes in use: kx columns and threads per y/z block of the
+    // inverse passes, the same of the forward passes, threads per x block
+    virtual void tiles(int *t5) const = 0;
     // axes whose passes classify band elements at compile time (x 1, y 2, z 4)
     virtual int band_axes() const = 0;
     // records that steps enqueued earlier (a replayed ensemble graph) ran

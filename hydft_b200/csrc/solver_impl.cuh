@@ -427,8 +427,10 @@ public:
     // (HYDFT_BAND=0 selects the runtime test everywhere)
     bool band_x = false, band_y = false, band_z = false;
     // tile shapes picked by tune(): kx columns per y/z block, threads per x block
-    int yz_tx = sizeof(R) == 4 ? 16 : 8;
+    int yz_tx = sizeof(R) == 4 ? 16 : 8;      // inverse y/z passes
     int yz_nt = sizeof(R) == 4 ? 256 : 128;
+    int yz_txf = sizeof(R) == 4 ? 16 : 8;     // forward y/z passes
+    int yz_ntf = sizeof(R) == 4 ? 256 : 128;
     int x_ntmax = 256;
     bool tuned = false;
     size_t alloc_bytes = 0;      // device memory allocated by this solver
@@ -741,13 +743,14 @@ public:
     // 256-point plan alone uses: a block then also spans two rows of the
     // other axis, or 32 columns)
     template <class F>
-    void with_yz(F &&f) const
+    void with_yz(bool fwd, F &&f) const
     {
+        const int tx = fwd ? yz_txf : yz_tx, ntb = fwd ? yz_ntf : yz_nt;
         auto nt = [&](auto TXc) {
-            if (yz_nt == 2 * YZ_NT) f(TXc, std::integral_constant<int, 2 * YZ_NT>{});
+            if (ntb == 2 * YZ_NT) f(TXc, std::integral_constant<int, 2 * YZ_NT>{});
             else f(TXc, std::integral_constant<int, YZ_NT>{});
         };
-        if (yz_tx == 8) nt(std::integral_constant<int, 8>{});
+        if (tx == 8) nt(std::integral_constant<int, 8>{});
         else nt(std::integral_constant<int, 16>{});
     }
     // rows of the other axis per y/z block for T threads per column
@@ -781,6 +784,12 @@ public:
     void inverse_shared(int nzf, const cplx<R> *const *src, const int *ops, int nf, const int *ysrc,
                         const int *yops)
     {
+        // the y transforms run in the order of their ZI sources, so that the
+        // two reads of a shared ZI buffer follow each other (the second from
+        // L2); each still writes YI buffer j
+        int yord[MAXF];
+        for (int j = 0; j < nf; ++j) yord[j] = j;
+        std::stable_sort(yord, yord + nf, [&](int a, int b) { return ysrc[a] < ysrc[b]; });
         PassArgs<R> a;
         a.nf = nzf;
         for (int f = 0; f < nzf; ++f) {
@@ -791,7 +800,7 @@ public:
         const double zbytes = nzf * cb() * g.nkxc * g.nkyc * (double)(g.nkzc + g.nz);
         const bool zf = with_plan(g.nz, [&](auto Tc, auto Ec) {
             constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value;
-            with_yz([&](auto TXc, auto NTc) {
+            with_yz(false, [&](auto TXc, auto NTc) {
             constexpr int TX = decltype(TXc)::value;
             constexpr int G = yz_rows<T, TX, decltype(NTc)::value>();
             const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
@@ -810,14 +819,15 @@ public:
             PassArgs<R> b;
             b.nf = nf;
             for (int f = 0; f < nf; ++f) {
-                b.in[f] = zi + (size_t)ysrc[f] * zsize;
-                b.out[f] = yi + (size_t)f * ysize;
-                b.op[f] = yops[f];
+                const int j = yord[f];
+                b.in[f] = zi + (size_t)ysrc[j] * zsize;
+                b.out[f] = yi + (size_t)j * ysize;
+                b.op[f] = yops[j];
             }
             const double ybytes = nf * cb() * g.nkxc * g.nz * (double)(g.nkyc + g.ny);
             const bool yf = with_plan(g.ny, [&](auto Tc, auto Ec) {
                 constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value;
-                with_yz([&](auto TXc, auto NTc) {
+                with_yz(false, [&](auto TXc, auto NTc) {
                 constexpr int TX = decltype(TXc)::value;
                 constexpr int G = yz_rows<T, TX, decltype(NTc)::value>();
                 const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
@@ -851,7 +861,7 @@ public:
             const double ybytes = nf * cb() * g.nkxc * g.nz * (double)(g.nkyc + g.ny);
             const bool yf = with_plan(g.ny, [&](auto Tc, auto Ec) {
                 constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value;
-                with_yz([&](auto TXc, auto NTc) {
+                with_yz(true, [&](auto TXc, auto NTc) {
                 constexpr int TX = decltype(TXc)::value;
                 constexpr int G = yz_rows<T, TX, decltype(NTc)::value>();
                 const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
@@ -878,7 +888,7 @@ public:
         const double zbytes = nf * cb() * g.nkxc * g.nkyc * (double)(g.nkzc + g.nz);
         const bool zf = with_plan(g.nz, [&](auto Tc, auto Ec) {
             constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value;
-            with_yz([&](auto TXc, auto NTc) {
+            with_yz(true, [&](auto TXc, auto NTc) {
             constexpr int TX = decltype(TXc)::value;
             constexpr int G = yz_rows<T, TX, decltype(NTc)::value>();
             const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
@@ -1335,11 +1345,13 @@ public:
 
     int prepare() override { return tune(); }
 
-    void tiles(int *yz, int *xnt, int *yznt) const override
+    void tiles(int *t) const override
     {
-        *yz = yz_tx;
-        *xnt = x_ntmax;
-        *yznt = yz_nt;
+        t[0] = yz_tx;
+        t[1] = yz_nt;
+        t[2] = yz_txf;
+        t[3] = yz_ntf;
+        t[4] = x_ntmax;
     }
 
     int band_axes() const override { return (band_x ? 1 : 0) | (band_y ? 2 : 0) | (band_z ? 4 : 0); }
@@ -1433,7 +1445,7 @@ public:
     // Autotuner of the tile shapes: times the phase-B transform sequence
     // (y/z inverse of its inputs, x pass B, y/z forward of its outputs) with
     // each candidate shape on the current data, writing only work buffers,
-    // and keeps the fastest.  Every shape gives the same results to the bit
+    // and keeps for each of the three groups the shape that ran it fastest.  Every shape gives the same results to the bit
     // (the same arithmetic per element, only the blocking differs).  The
     // choice is shared by every model of the same grid, precision and
     // physics in the process.  HYDFT_TUNE=0 keeps the defaults.
@@ -1444,10 +1456,11 @@ public:
             return std::tie(nx, ny, nz, bytes, nm, evolve, ext) < std::tie(o.nx, o.ny, o.nz, o.bytes, o.nm, o.evolve, o.ext);
         }
     };
-    // cached shape: {kx columns per y/z block, threads per y/z block, threads per x block}
-    static std::map<TuneKey, std::array<int, 3>> &tune_cache()
+    // cached shape: kx columns and threads per y/z block of the inverse and
+    // of the forward passes, threads per x block
+    static std::map<TuneKey, std::array<int, 5>> &tune_cache()
     {
-        static std::map<TuneKey, std::array<int, 3>> m;
+        static std::map<TuneKey, std::array<int, 5>> m;
         return m;
     }
     static std::mutex &tune_mutex()
@@ -1467,9 +1480,9 @@ public:
         const char *fy = std::getenv("HYDFT_YZ_TILE"), *fx = std::getenv("HYDFT_X_THREADS");
         const char *fn = std::getenv("HYDFT_YZ_THREADS");
         if ((fy && *fy) || (fx && *fx) || (fn && *fn)) {
-            if (fy && (std::string(fy) == "8" || std::string(fy) == "16")) yz_tx = std::atoi(fy);
+            if (fy && (std::string(fy) == "8" || std::string(fy) == "16")) yz_tx = yz_txf = std::atoi(fy);
             if (fx && (std::string(fx) == "128" || std::string(fx) == "256")) x_ntmax = std::atoi(fx);
-            if (fn && (std::atoi(fn) == YZ_NT || std::atoi(fn) == 2 * YZ_NT)) yz_nt = std::atoi(fn);
+            if (fn && (std::atoi(fn) == YZ_NT || std::atoi(fn) == 2 * YZ_NT)) yz_nt = yz_ntf = std::atoi(fn);
             return 0;
         }
         if (!(has_plan(g.ny) || has_plan(g.nz))) return 0;
@@ -1480,7 +1493,9 @@ public:
             if (it != tune_cache().end()) {
                 yz_tx = it->second[0];
                 yz_nt = it->second[1];
-                x_ntmax = it->second[2];
+                yz_txf = it->second[2];
+                yz_ntf = it->second[3];
+                x_ntmax = it->second[4];
                 return 0;
             }
         }
@@ -1500,53 +1515,62 @@ public:
         pw.stage = 0;
         pw.status = &ctrl->status;
         const int64_t launches0 = launches;
-        cudaEvent_t e0, e1;
-        CK(cudaEventCreate(&e0));
-        CK(cudaEventCreate(&e1));
-        auto time_it = [&](int tx, int ynt, int ntmax) -> float {
-            yz_tx = tx;
-            yz_nt = ynt;
+        cudaEvent_t tev[4];
+        for (auto &e : tev) CK(cudaEventCreate(&e));
+        // one candidate: the inverse, x and forward groups timed apart (best
+        // of two runs after a warm-up), so that each group's shape is chosen
+        // by its own time
+        auto time_it = [&](int tx, int ynt, int ntmax, float (&ms)[3]) {
+            yz_tx = yz_txf = tx;
+            yz_nt = yz_ntf = ynt;
             x_ntmax = ntmax;
-            float best = 1e30f;
+            for (float &m : ms) m = 1e30f;
             for (int rep = 0; rep < 3; ++rep) {
-                cudaEventRecord(e0, st);
+                cudaEventRecord(tev[0], st);
                 bool dxp = false;
                 const int nf = phase_b_inverse(dxp);
+                cudaEventRecord(tev[1], st);
                 if (fast_x) xb_launch(nf, nout, pw, ph.evolve ? 1 + nm : 1, dxp);
                 else xpass(nf, nout, pw, xrb_b, "xpass_b", ph.evolve ? 1 + nm : 1);
+                cudaEventRecord(tev[2], st);
                 forward(nout, OB);
-                cudaEventRecord(e1, st);
-                cudaEventSynchronize(e1);
-                float ms = 0.f;
-                cudaEventElapsedTime(&ms, e0, e1);
-                if (rep > 0) best = std::min(best, ms);   // the first run warms up
+                cudaEventRecord(tev[3], st);
+                cudaEventSynchronize(tev[3]);
+                for (int k = 0; k < 3; ++k) {
+                    float t = 0.f;
+                    cudaEventElapsedTime(&t, tev[k], tev[k + 1]);
+                    if (rep > 0) ms[k] = std::min(ms[k], t);   // the first run warms up
+                }
             }
-            return best;
         };
         const int txs[2] = {8, 16};
         const int nts[2] = {128, 256};
         const int ynts[2] = {YZ_NT, 2 * YZ_NT};
         // the wide y/z blocks exist for the 256-point plan only
         const bool wide = g.ny == 256 || g.nz == 256;
-        float best = 1e30f;
-        int btx = yz_tx, bynt = yz_nt, bnt = x_ntmax;
+        float bi = 1e30f, bx = 1e30f, bf = 1e30f;
+        int btx = yz_tx, bynt = yz_nt, btxf = yz_txf, byntf = yz_ntf, bnt = x_ntmax;
         for (int tx : txs)
             for (int ynt : ynts)
                 for (int nt : nts) {
                     if (!fast_x && nt != 256) continue;
                     if (!wide && ynt != YZ_NT) continue;
-                    const float ms = time_it(tx, ynt, nt);
-                    if (ms < best) { best = ms; btx = tx; bynt = ynt; bnt = nt; }
+                    float ms[3];
+                    time_it(tx, ynt, nt, ms);
+                    if (ms[0] < bi) { bi = ms[0]; btx = tx; bynt = ynt; }
+                    if (ms[1] < bx) { bx = ms[1]; bnt = nt; }
+                    if (ms[2] < bf) { bf = ms[2]; btxf = tx; byntf = ynt; }
                 }
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
+        for (auto &e : tev) cudaEventDestroy(e);
         launches = launches0;
         yz_tx = btx;
         yz_nt = bynt;
+        yz_txf = btxf;
+        yz_ntf = byntf;
         x_ntmax = bnt;
         CK(cudaGetLastError());
         std::lock_guard<std::mutex> lk(tune_mutex());
-        tune_cache()[key] = {btx, bynt, bnt};
+        tune_cache()[key] = {btx, bynt, btxf, byntf, bnt};
         return 0;
     }
 

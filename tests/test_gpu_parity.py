@@ -315,6 +315,7 @@ def test_tile_shapes_give_identical_results(hg, monkeypatch):
     m.set_state(n, mom, pi)
     m.advance(3)
     assert m.scalar("yz_tile") in (8, 16) and m.scalar("x_threads") in (128, 256)
+    assert m.scalar("yz_tile_fwd") in (8, 16)
     for x, y in zip(m.get_state(), out[0]):
         assert np.array_equal(x, y)
 
@@ -361,6 +362,7 @@ def test_wide_yz_blocks_give_identical_results(hg, monkeypatch, prec, base):
         m.set_state(n, mom, pi)
         m.advance(2)
         assert m.scalar("yz_tile") == int(tile) and m.scalar("yz_threads") == nt
+        assert m.scalar("yz_tile_fwd") == int(tile) and m.scalar("yz_threads_fwd") == nt
         out.append(m.get_state())
         m.close()
     for other in out[1:]:
