@@ -1479,10 +1479,19 @@ public:
         // YZ_NT | 2 YZ_NT, HYDFT_X_THREADS = 128 | 256)
         const char *fy = std::getenv("HYDFT_YZ_TILE"), *fx = std::getenv("HYDFT_X_THREADS");
         const char *fn = std::getenv("HYDFT_YZ_THREADS");
-        if ((fy && *fy) || (fx && *fx) || (fn && *fn)) {
-            if (fy && (std::string(fy) == "8" || std::string(fy) == "16")) yz_tx = yz_txf = std::atoi(fy);
+        // HYDFT_YZ_TILE_FWD / HYDFT_YZ_THREADS_FWD: the forward passes' shape alone
+        const char *gy = std::getenv("HYDFT_YZ_TILE_FWD"), *gn = std::getenv("HYDFT_YZ_THREADS_FWD");
+        auto set = [](const char *e) { return e && *e; };
+        if (set(fy) || set(fx) || set(fn) || set(gy) || set(gn)) {
+            auto tile = [](const char *e, int &a) { if (e && (std::atoi(e) == 8 || std::atoi(e) == 16)) a = std::atoi(e); };
+            auto nthr = [](const char *e, int &a) { if (e && (std::atoi(e) == YZ_NT || std::atoi(e) == 2 * YZ_NT)) a = std::atoi(e); };
+            tile(fy, yz_tx);
+            tile(fy, yz_txf);
+            tile(gy, yz_txf);
+            nthr(fn, yz_nt);
+            nthr(fn, yz_ntf);
+            nthr(gn, yz_ntf);
             if (fx && (std::string(fx) == "128" || std::string(fx) == "256")) x_ntmax = std::atoi(fx);
-            if (fn && (std::atoi(fn) == YZ_NT || std::atoi(fn) == 2 * YZ_NT)) yz_nt = yz_ntf = std::atoi(fn);
             return 0;
         }
         if (!(has_plan(g.ny) || has_plan(g.nz))) return 0;
