@@ -5,7 +5,8 @@
  * pseudo-spectral solver step (abdoudiaw/HyDFT, Fortran 2018) and of the setup
  * pieces it depends on.  It exists to check the CUDA product path: only the
  * tests, the smoke check and the CPU-baseline leg of the benchmark may load
- * it, and only as the checker.  Nothing in the product links or calls it.
+ * it, and only as the reference the device results are compared with.
+ * Nothing in the product links or calls it.
  *
  * It follows the reference's operator sequence literally (every spectral
  * operator does its own FFT round trip, exactly as src/core/spectral.f90 does),

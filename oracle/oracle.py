@@ -2,7 +2,8 @@
 
 The oracle is a plain-C FP64 restatement of the HyDFT solver step (see
 oracle/oracle.h).  Only the tests, the smoke check and the CPU-baseline leg of
-the benchmark use this module, and only as the checker.
+the benchmark use this module, and only as the reference the device results
+are compared with.
 
 Arrays follow the reference's Fortran layout: a field u(nx,ny,nz) is a numpy
 array of shape (nz, ny, nx) in C order; a half spectrum has shape

@@ -1,6 +1,6 @@
 """The reference's own known-answer tests, restated against the CPU oracle
 with the reference's thresholds.  These pin the oracle before it is trusted
-as the checker of the CUDA path.
+as the reference for the CUDA path.
 
   test/test_fft.f90:21-52        FFT round trip and normalised amplitudes
   test/test_ops.f90:30-71        derivatives, Laplacian, div, convolution, dealias
