@@ -31,7 +31,6 @@ struct PassArgs {
     const cplx<R> *in[MAXF];
     cplx<R> *out[MAXF];
     int op[MAXF];
-    int lo, hi;   // y passes (register plans): the z planes [lo, hi) this launch covers
 };
 
 // twiddle tables exp(-2 pi i t/L), t < L, for the three axes

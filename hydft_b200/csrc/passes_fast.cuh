@@ -188,8 +188,8 @@ __global__ void __launch_bounds__(TX * T * G) yinv_fast(Grid g, PassArgs<R> a, c
     cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
     cplx<R> *xb = tw + 2 * L;
     const int tid = threadIdx.x, c = tid % TX, t = (tid / TX) % T, gi = tid / (TX * T);
-    const int x = blockIdx.x * TX + c, z = a.lo + blockIdx.y * G + gi, f = blockIdx.z;
-    const bool valid = x < g.nkxc && z < a.hi;
+    const int x = blockIdx.x * TX + c, z = blockIdx.y * G + gi, f = blockIdx.z;
+    const bool valid = x < g.nkxc && z < g.nz;
     for (int i = tid; i < 2 * L; i += blockDim.x) tw[i] = twy[i];
     cplx<R> v[E];
     load_band<R, T, E, BAND>(v, a.in[f] + (size_t)z * g.nkyc * g.pkx + x, g.pkx, t, g.My, g.nkyc, valid);
@@ -214,8 +214,8 @@ __global__ void __launch_bounds__(TX * T * G) yfwd_fast(Grid g, PassArgs<R> a, c
     cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
     cplx<R> *xb = tw + 2 * L;
     const int tid = threadIdx.x, c = tid % TX, t = (tid / TX) % T, gi = tid / (TX * T);
-    const int x = blockIdx.x * TX + c, z = a.lo + blockIdx.y * G + gi, f = blockIdx.z;
-    const bool valid = x < g.nkxc && z < a.hi;
+    const int x = blockIdx.x * TX + c, z = blockIdx.y * G + gi, f = blockIdx.z;
+    const bool valid = x < g.nkxc && z < g.nz;
     for (int i = tid; i < 2 * L; i += blockDim.x) tw[i] = twy[i];
     cplx<R> v[E];
     load_block<R, T, E>(v, a.in[f] + (size_t)z * g.ny * g.pkx + x, g.pkx, t, valid);
@@ -371,7 +371,6 @@ struct XFastArgs {
     cplx<R> *out[MAXF];
     int nin, nout;
     int dx_in_pass;   // phase B (xb_rows): the x derivatives arrive underived
-    int row_lo, row_hi;   // xa_regs / xb_rows: the rows (y + ny z) [row_lo, row_hi) of this launch
 };
 
 // packed (i <= j) flux index -> (i, j) for three components
@@ -645,9 +644,9 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xa_regs(Grid g, XFa
     cplx<R> *sb = tw + 2 * L;                      // [4][rb][pkx] the staged inputs
     cplx<R> *xbuf = sb + 4 * (size_t)rb * pk;
     const int tid = threadIdx.x, t = tid % T, rr = tid / T;
-    const int row0 = a.row_lo + blockIdx.x * rb, row = row0 + rr;
-    const bool rowok = row < a.row_hi;
-    const int vrows = max(0, min(rb, a.row_hi - row0));
+    const int row0 = blockIdx.x * rb, row = row0 + rr;
+    const bool rowok = row < g.ny * g.nz;
+    const int vrows = max(0, min(rb, g.ny * g.nz - row0));
     cplx<R> *xrow = xbuf + rr * xrow_stride<T, E>();
     // the block's rows of all four inputs on their way at once, one commit
     // group per pair: pair 1 lands while pair 0 is transformed
@@ -765,8 +764,8 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xb_rows(Grid g, XFa
     cplx<R> *xbuf = sb + 2 * (size_t)rb * pk;
     R *rs = reinterpret_cast<R *>(xbuf + rb * xrow_stride<T, E>());   // [3][rb][RS] u rows
     const int tid = threadIdx.x, t = tid % T, rr = tid / T;
-    const int nrows = a.row_hi;
-    const int row0 = a.row_lo + blockIdx.x * rb;
+    const int nrows = g.ny * g.nz;
+    const int row0 = blockIdx.x * rb;
     const int row = row0 + rr;
     const bool rowok = row < nrows;
     cplx<R> *xrow = xbuf + rr * xrow_stride<T, E>();

@@ -390,17 +390,6 @@ public:
     size_t csize, zsize, ysize, ncell;
     int nin_max, nout_max;
     cudaStream_t st = nullptr;
-    // the y/x/y chain of a phase as two halves of the z planes (HYDFT_SPLIT=1):
-    // the second half runs on st2 (forked from and joined back to st), so
-    // that one half's issue-bound x pass can overlap the other half's y
-    // passes.  Off by default: at 256^3 the x blocks fill each SM's shared
-    // memory, the overlap only displaces them and the step is slower.  ls is
-    // the stream and [zlo, zhi) the z planes of the y and x launches being
-    // issued (st and all planes outside yx_halves).
-    cudaStream_t st2 = nullptr, ls = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-    int zlo = 0, zhi = 0;
-    bool split_yx = false;   // HYDFT_SPLIT=1: the two-stream halves (slower at 256^3)
     std::vector<void *> allocs;
     // compact fields
     cplx<R> *N, *M[3], *P[6], *RN, *RM[3], *RP[6], *P0[6], *MU, *Q[3];
@@ -507,9 +496,6 @@ public:
         if (gexec) cudaGraphExecDestroy(gexec);
         if (graph) cudaGraphDestroy(graph);
         for (void *p : allocs) cudaFree(p);
-        if (ev_fork) cudaEventDestroy(ev_fork);
-        if (ev_join) cudaEventDestroy(ev_join);
-        if (st2) cudaStreamDestroy(st2);
         if (st) cudaStreamDestroy(st);
     }
 
@@ -536,16 +522,6 @@ public:
         device = dev;
         CK(cudaSetDevice(dev));
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-        CK(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
-        CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
-        CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
-        ls = st;
-        zlo = 0;
-        zhi = s.g.nz;
-        {
-            const char *sp = std::getenv("HYDFT_SPLIT");
-            if (sp && std::string(sp) == "1") split_yx = true;
-        }
         int optin = 0;
         CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
         smem_optin = optin;
@@ -808,13 +784,12 @@ public:
     void inverse_shared(int nzf, const cplx<R> *const *src, const int *ops, int nf, const int *ysrc,
                         const int *yops)
     {
-        zinv_stage(nzf, src, ops);
-        yinv_stage(nf, ysrc, yops);
-    }
-
-    // the z part of inverse_shared (all planes, on st)
-    void zinv_stage(int nzf, const cplx<R> *const *src, const int *ops)
-    {
+        // the y transforms run in the order of their ZI sources, so that the
+        // two reads of a shared ZI buffer follow each other (the second from
+        // L2); each still writes YI buffer j
+        int yord[MAXF];
+        for (int j = 0; j < nf; ++j) yord[j] = j;
+        std::stable_sort(yord, yord + nf, [&](int a, int b) { return ysrc[a] < ysrc[b]; });
         PassArgs<R> a;
         a.nf = nzf;
         for (int f = 0; f < nzf; ++f) {
@@ -840,29 +815,16 @@ public:
             const size_t smz = sizeof(cplx<R>) * (2 * (size_t)g.nz * TX + g.nz);
             launch("zinv", zbytes, [&] { zinv_kernel<R, TX><<<dim3(ntx, g.nkyc, nzf), 256, smz, st>>>(g, a, twz); });
         }
-    }
-
-    // the y part of inverse_shared: planes [zlo, zhi) on ls
-    void yinv_stage(int nf, const int *ysrc, const int *yops)
-    {
-        // the y transforms run in the order of their ZI sources, so that the
-        // two reads of a shared ZI buffer follow each other (the second from
-        // L2); each still writes YI buffer j
-        int yord[MAXF];
-        for (int j = 0; j < nf; ++j) yord[j] = j;
-        std::stable_sort(yord, yord + nf, [&](int a, int b) { return ysrc[a] < ysrc[b]; });
         if (g.ny > 1) {
             PassArgs<R> b;
             b.nf = nf;
-            b.lo = zlo;
-            b.hi = zhi;
             for (int f = 0; f < nf; ++f) {
                 const int j = yord[f];
                 b.in[f] = zi + (size_t)ysrc[j] * zsize;
                 b.out[f] = yi + (size_t)j * ysize;
                 b.op[f] = yops[j];
             }
-            const double ybytes = nf * cb() * g.nkxc * (double)(zhi - zlo) * (g.nkyc + g.ny);
+            const double ybytes = nf * cb() * g.nkxc * g.nz * (double)(g.nkyc + g.ny);
             const bool yf = with_plan(g.ny, [&](auto Tc, auto Ec) {
                 constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value;
                 with_yz(false, [&](auto TXc, auto NTc) {
@@ -871,14 +833,14 @@ public:
                 const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
                 auto k = band_y ? yinv_fast<R, T, E, TX, G, true> : yinv_fast<R, T, E, TX, G, false>;
                 set_smem(k, sm);
-                const dim3 grid((g.nkxc + TX - 1) / TX, (zhi - zlo + G - 1) / G, nf);
-                launch("yinv", ybytes, [&] { k<<<grid, TX * T * G, sm, ls>>>(g, b, tpy); });
+                const dim3 grid((g.nkxc + TX - 1) / TX, (g.nz + G - 1) / G, nf);
+                launch("yinv", ybytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, b, tpy); });
             });
             });
             if (!yf) {
                 const int ntx = (g.nkxc + TX - 1) / TX;
                 const size_t smy = sizeof(cplx<R>) * (2 * (size_t)g.ny * TX + g.ny);
-                launch("yinv", ybytes, [&] { yinv_kernel<R, TX><<<dim3(ntx, g.nz, nf), 256, smy, ls>>>(g, b, twy); });
+                launch("yinv", ybytes, [&] { yinv_kernel<R, TX><<<dim3(ntx, g.nz, nf), 256, smy, st>>>(g, b, twy); });
             }
         }
     }
@@ -886,25 +848,17 @@ public:
     // forward transform of the x-pass outputs 0..nf-1 into compact fields
     void forward(int nf, cplx<R> *const *dst)
     {
-        yfwd_stage(nf);
-        zfwd_stage(nf, dst);
-    }
-
-    // the y part of forward: planes [zlo, zhi) on ls
-    void yfwd_stage(int nf)
-    {
         const int ntx = (g.nkxc + TX - 1) / TX;
+        const cplx<R> *src = xo;
         if (g.ny > 1) {
             PassArgs<R> b;
             b.nf = nf;
-            b.lo = zlo;
-            b.hi = zhi;
             for (int f = 0; f < nf; ++f) {
                 b.in[f] = xo + (size_t)f * ysize;
                 b.out[f] = zi + (size_t)f * zsize;
                 b.op[f] = OP_ID;
             }
-            const double ybytes = nf * cb() * g.nkxc * (double)(zhi - zlo) * (g.nkyc + g.ny);
+            const double ybytes = nf * cb() * g.nkxc * g.nz * (double)(g.nkyc + g.ny);
             const bool yf = with_plan(g.ny, [&](auto Tc, auto Ec) {
                 constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value;
                 with_yz(true, [&](auto TXc, auto NTc) {
@@ -913,22 +867,16 @@ public:
                 const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
                 auto k = band_y ? yfwd_fast<R, T, E, TX, G, true> : yfwd_fast<R, T, E, TX, G, false>;
                 set_smem(k, sm);
-                const dim3 grid((g.nkxc + TX - 1) / TX, (zhi - zlo + G - 1) / G, nf);
-                launch("yfwd", ybytes, [&] { k<<<grid, TX * T * G, sm, ls>>>(g, b, tpy); });
+                const dim3 grid((g.nkxc + TX - 1) / TX, (g.nz + G - 1) / G, nf);
+                launch("yfwd", ybytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, b, tpy); });
             });
             });
             if (!yf) {
                 const size_t smy = sizeof(cplx<R>) * (2 * (size_t)g.ny * TX + g.ny);
-                launch("yfwd", ybytes, [&] { yfwd_kernel<R, TX><<<dim3(ntx, g.nz, nf), 256, smy, ls>>>(g, b, twy); });
+                launch("yfwd", ybytes, [&] { yfwd_kernel<R, TX><<<dim3(ntx, g.nz, nf), 256, smy, st>>>(g, b, twy); });
             }
+            src = zi;
         }
-    }
-
-    // the z part of forward (all planes, on st)
-    void zfwd_stage(int nf, cplx<R> *const *dst)
-    {
-        const int ntx = (g.nkxc + TX - 1) / TX;
-        const cplx<R> *src = g.ny > 1 ? zi : xo;
         PassArgs<R> a;
         a.nf = nf;
         for (int f = 0; f < nf; ++f) {
@@ -977,8 +925,6 @@ public:
         a.nin = nin;
         a.nout = nout;
         a.dx_in_pass = 0;
-        a.row_lo = zlo * g.ny;
-        a.row_hi = zhi * g.ny;
         for (int f = 0; f < nin; ++f) a.in[f] = yi + (size_t)f * ysize;
         for (int f = 0; f < nout; ++f) a.out[f] = xo + (size_t)f * ysize;
         return a;
@@ -1014,9 +960,8 @@ public:
                     sm = xstaged_smem<R, T, E>(nt, g.pkx, 4, 0);
                 }
                 set_smem(k, sm);
-                const int rb = nt / T, rows = a.row_hi - a.row_lo;
-                launch(name, xbytes(nin, nout, nreal) * rows / nrows,
-                       [&] { k<<<(rows + rb - 1) / rb, nt, sm, ls>>>(g, a, tpx, pw); });
+                const int rb = nt / T;
+                launch(name, xbytes(nin, nout, nreal), [&] { k<<<(nrows + rb - 1) / rb, nt, sm, st>>>(g, a, tpx, pw); });
             };
             const bool no_fd = !ph.has_tf && !ph.has_grad;
             if (staged_x && uonly) {
@@ -1056,9 +1001,8 @@ public:
                     sm = xstaged_smem<R, T, E>(nt, g.pkx, 2, nreal_rows);
                 }
                 set_smem(k, sm);
-                const int rb = nt / T, rows = a.row_hi - a.row_lo;
-                launch("xpass_b", xbytes(nin, nout, nreal) * rows / nrows,
-                       [&] { k<<<(rows + rb - 1) / rb, nt, sm, ls>>>(g, a, tpx, pw); });
+                const int rb = nt / T;
+                launch("xpass_b", xbytes(nin, nout, nreal), [&] { k<<<(nrows + rb - 1) / rb, nt, sm, st>>>(g, a, tpx, pw); });
             };
             const int extk = !ph.ext_active ? 0 : (ph.ext_kind == 3 ? 2 : 1);
             auto rows = [&](auto ev, auto ek) {
@@ -1133,37 +1077,6 @@ public:
     }
 
     // -------------------------------------------------------------- stage
-    // f() issues a phase's y inverse, x pass and y forward.  With the split
-    // on (3-D, register plans on y, the staged x passes; not while profiling
-    // per kernel) it runs twice: planes [0, nz/2) on st, then
-    // [nz/2, nz) on st2, forked after everything issued so far and joined
-    // before anything issued after; the halves touch disjoint planes of YI,
-    // XO, ZI and the real fields.  Otherwise once over all planes on st.
-    template <class F>
-    void yx_halves(bool ok, F &&f)
-    {
-        ls = st;
-        zlo = 0;
-        zhi = g.nz;
-        if (!(ok && split_yx && !profiling && g.nz >= 2 && g.ny > 1 && has_plan(g.ny))) {
-            f();
-            return;
-        }
-        const int h = g.nz / 2;
-        cudaEventRecord(ev_fork, st);
-        cudaStreamWaitEvent(st2, ev_fork, 0);
-        zhi = h;
-        f();
-        ls = st2;
-        zlo = h;
-        zhi = g.nz;
-        f();
-        cudaEventRecord(ev_join, st2);
-        cudaStreamWaitEvent(st, ev_join, 0);
-        ls = st;
-        zlo = 0;
-    }
-
     void phase_a(int stage, bool write_u)
     {
         const cplx<R> *src[MAXF];
@@ -1175,9 +1088,7 @@ public:
             for (int d = 0; d < nm; ++d) { src[nf] = N; ops[nf++] = OP_IKX + d; }
             src[nf] = N; ops[nf++] = OP_NK2;
         }
-        zinv_stage(nf, src, ops);
-        int ysrc[MAXF], yops[MAXF];
-        for (int f = 0; f < nf; ++f) { ysrc[f] = f; yops[f] = OP_ID; }
+        inverse(nf, src, ops);
         PWA<R> pw;
         pw.ph = ph;
         pw.nm = nm;
@@ -1189,15 +1100,9 @@ public:
         pw.ncell = ncell;
         pw.status = &ctrl->status;
         const int nout = nm + nm * (nm + 1) / 2 + 1;
-        // xa_regs (the staged pass) takes a row range
-        const bool staged = fast_x && staged_x && !ph.has_grad && !ph.has_tf;
-        yx_halves(staged, [&] {
-            yinv_stage(nf, ysrc, yops);
-            if (fast_x) xa_launch(nf, nout, pw, ph.has_grad != 0, false, "xpass_a", write_u ? 1 + nm : 1);
-            else xpass(nf, nout, pw, xrb_a, "xpass_a", write_u ? 1 + nm : 1);
-            yfwd_stage(nout);
-        });
-        zfwd_stage(nout, OA);
+        if (fast_x) xa_launch(nf, nout, pw, ph.has_grad != 0, false, "xpass_a", write_u ? 1 + nm : 1);
+        else xpass(nf, nout, pw, xrb_a, "xpass_a", write_u ? 1 + nm : 1);
+        forward(nout, OA);
         CombineA<R> c;
         c.N = N;
         for (int d = 0; d < 3; ++d) c.M[d] = M[d];
@@ -1221,22 +1126,12 @@ public:
     // not three times.
     int phase_b_inverse(bool &dx_in_pass)
     {
-        int ysrc[MAXF], yops[MAXF];
-        const int nf = phase_b_zinv(dx_in_pass, ysrc, yops);
-        yinv_stage(nf, ysrc, yops);
-        return nf;
-    }
-
-    // the z stage of phase_b_inverse; fills the y stage's list (ysrc, yops)
-    // and returns its length
-    int phase_b_zinv(bool &dx_in_pass, int *ysrc, int *yops)
-    {
         const cplx<R> *src[MAXF];
         int ops[MAXF];
         int nf = 0;
         dx_in_pass = fast_x && staged_x && g.ny > 1 && has_plan(g.ny);
         if (dx_in_pass) {
-            int nzf = 0;
+            int nzf = 0, ysrc[MAXF], yops[MAXF];
             auto field = [&](const cplx<R> *f) {
                 const int z0 = nzf;
                 src[nzf] = f; ops[nzf++] = OP_ID;
@@ -1259,15 +1154,14 @@ public:
                             yops[nf++] = d == 1 ? OP_IKY : OP_ID;
                         }
             }
-            zinv_stage(nzf, src, ops);
+            inverse_shared(nzf, src, ops, nf, ysrc, yops);
         } else {
             for (int d = 0; d < nm; ++d) { src[nf] = MU; ops[nf++] = OP_IKX + d; }
             if (ph.evolve)
                 for (int cp = 0; cp < 3; ++cp)
                     for (int d = 0; d < nm; ++d)
                         for (int h = 0; h < 2; ++h) { src[nf] = P[2 * cp + h]; ops[nf++] = OP_IKX + d; }
-            zinv_stage(nf, src, ops);
-            for (int f = 0; f < nf; ++f) { ysrc[f] = f; yops[f] = OP_ID; }
+            inverse(nf, src, ops);
         }
         return nf;
     }
@@ -1275,8 +1169,7 @@ public:
     void phase_b(int stage, bool rhs_only)
     {
         bool dxp = false;
-        int ysrc[MAXF], yops[MAXF];
-        const int nf = phase_b_zinv(dxp, ysrc, yops);
+        const int nf = phase_b_inverse(dxp);
         PWB<R> pw;
         pw.ph = ph;
         pw.nm = nm;
@@ -1298,13 +1191,9 @@ public:
             });
             launch("force_mean", 0.0, [&] { gauss_force_final_kernel<<<1, 32, 0, st>>>(spart, red_blocks, ctrl); });
         }
-        yx_halves(fast_x && staged_x, [&] {
-            yinv_stage(nf, ysrc, yops);
-            if (fast_x) xb_launch(nf, nout, pw, ph.evolve ? 1 + nm : 1, dxp);
-            else xpass(nf, nout, pw, xrb_b, "xpass_b", ph.evolve ? 1 + nm : 1);
-            yfwd_stage(nout);
-        });
-        zfwd_stage(nout, OB);
+        if (fast_x) xb_launch(nf, nout, pw, ph.evolve ? 1 + nm : 1, dxp);
+        else xpass(nf, nout, pw, xrb_b, "xpass_b", ph.evolve ? 1 + nm : 1);
+        forward(nout, OB);
         CombineB<R> c;
         c.N = N; c.RN = RN; c.oN = HN;
         for (int d = 0; d < 3; ++d) {

@@ -368,28 +368,3 @@ def test_wide_yz_blocks_give_identical_results(hg, monkeypatch, prec, base):
     for other in out[1:]:
         for x, y in zip(out[0], other):
             assert np.array_equal(x, y)
-
-
-@pytest.mark.parametrize("closure,prec", [("maxwell", "fp32"), ("newtonian", "fp64")])
-def test_split_halves_give_identical_results(hg, monkeypatch, closure, prec):
-    """Each phase's y inverse, x pass and y forward can run as two halves of the
-    z planes on two streams when HYDFT_SPLIT=1; the halves write disjoint
-    planes, so the fields equal those of one stream over all planes
-    (HYDFT_SPLIT=0, the default) to the bit, through the captured step graph
-    and through the eager rhs."""
-    kw = dict(ION, nx=64, ny=64, nz=48, lx=32.0, ly=32.0, lz=24.0, closure=closure, tau_model="constant",
-              tau=1.5, dt=0.01, gpu_precision=prec)
-    out, rhs = [], []
-    for flag in ("0", "1"):
-        monkeypatch.setenv("HYDFT_SPLIT", flag)
-        m = hg.Model(hg.default_params(**kw))
-        n, mom, pi = seeded_state(m)
-        m.set_state(n, mom, pi)
-        rhs.append(m.rhs(0.0))
-        m.advance(3)
-        out.append(m.get_state())
-        m.close()
-    for a, b in zip(tuple(out[0]) + tuple(rhs[0]), tuple(out[1]) + tuple(rhs[1])):
-        if a is None:
-            continue
-        assert np.array_equal(a, b)
