@@ -739,7 +739,7 @@ public:
     static constexpr int YZ_TX = sizeof(R) == 4 ? 16 : 8;
 
     // the y/z passes' block shape as compile-time constants: kx columns per
-    // block (8 or 16) and threads per block (YZ_NT, or 2 YZ_NT, which the
+    // block (8, 16 or 32) and threads per block (YZ_NT, or 2 YZ_NT, which the
     // 256-point plan alone uses: a block then also spans two rows of the
     // other axis, or 32 columns)
     template <class F>
@@ -751,7 +751,8 @@ public:
             else f(TXc, std::integral_constant<int, YZ_NT>{});
         };
         if (tx == 8) nt(std::integral_constant<int, 8>{});
-        else nt(std::integral_constant<int, 16>{});
+        else if (tx == 16) nt(std::integral_constant<int, 16>{});
+        else nt(std::integral_constant<int, 32>{});
     }
     // rows of the other axis per y/z block for T threads per column
     template <int T, int TX, int NTR>
@@ -1475,7 +1476,7 @@ public:
         tuned = true;
         const char *ev = std::getenv("HYDFT_TUNE");
         if (ev && std::string(ev) == "0") return 0;
-        // fixed shapes on request (HYDFT_YZ_TILE = 8 | 16, HYDFT_YZ_THREADS =
+        // fixed shapes on request (HYDFT_YZ_TILE = 8 | 16 | 32, HYDFT_YZ_THREADS =
         // YZ_NT | 2 YZ_NT, HYDFT_X_THREADS = 128 | 256)
         const char *fy = std::getenv("HYDFT_YZ_TILE"), *fx = std::getenv("HYDFT_X_THREADS");
         const char *fn = std::getenv("HYDFT_YZ_THREADS");
@@ -1483,7 +1484,9 @@ public:
         const char *gy = std::getenv("HYDFT_YZ_TILE_FWD"), *gn = std::getenv("HYDFT_YZ_THREADS_FWD");
         auto set = [](const char *e) { return e && *e; };
         if (set(fy) || set(fx) || set(fn) || set(gy) || set(gn)) {
-            auto tile = [](const char *e, int &a) { if (e && (std::atoi(e) == 8 || std::atoi(e) == 16)) a = std::atoi(e); };
+            auto tile = [](const char *e, int &a) {
+                if (e && (std::atoi(e) == 8 || std::atoi(e) == 16 || std::atoi(e) == 32)) a = std::atoi(e);
+            };
             auto nthr = [](const char *e, int &a) { if (e && (std::atoi(e) == YZ_NT || std::atoi(e) == 2 * YZ_NT)) a = std::atoi(e); };
             tile(fy, yz_tx);
             tile(fy, yz_txf);
@@ -1552,7 +1555,7 @@ public:
                 }
             }
         };
-        const int txs[2] = {8, 16};
+        const int txs[3] = {8, 16, 32};
         const int nts[2] = {128, 256};
         const int ynts[2] = {YZ_NT, 2 * YZ_NT};
         // the wide y/z blocks exist for the 256-point plan only

@@ -295,7 +295,7 @@ def test_tile_shapes_give_identical_results(hg, monkeypatch):
     kw = dict(ION, nx=64, ny=32, nz=48, lx=32.0, ly=16.0, lz=24.0, closure="maxwell", tau_model="constant",
               tau=1.5, dt=0.01, gpu_precision="fp32")
     out = []
-    for tile, nt in (("8", "128"), ("16", "256"), ("8", "256")):
+    for tile, nt in (("8", "128"), ("16", "256"), ("8", "256"), ("32", "256")):
         monkeypatch.setenv("HYDFT_YZ_TILE", tile)
         monkeypatch.setenv("HYDFT_X_THREADS", nt)
         m = hg.Model(hg.default_params(**kw))
@@ -314,8 +314,8 @@ def test_tile_shapes_give_identical_results(hg, monkeypatch):
     n, mom, pi = seeded_state(m)
     m.set_state(n, mom, pi)
     m.advance(3)
-    assert m.scalar("yz_tile") in (8, 16) and m.scalar("x_threads") in (128, 256)
-    assert m.scalar("yz_tile_fwd") in (8, 16)
+    assert m.scalar("yz_tile") in (8, 16, 32) and m.scalar("x_threads") in (128, 256)
+    assert m.scalar("yz_tile_fwd") in (8, 16, 32)
     for x, y in zip(m.get_state(), out[0]):
         assert np.array_equal(x, y)
 
@@ -354,7 +354,7 @@ def test_wide_yz_blocks_give_identical_results(hg, monkeypatch, prec, base):
     kw = dict(ION, nx=32, ny=256, nz=256, lx=16.0, ly=128.0, lz=128.0, closure="maxwell", tau_model="constant",
               tau=1.5, dt=0.01, gpu_precision=prec)
     out = []
-    for tile, nt in (("16", base), ("16", 2 * base), ("8", 2 * base)):
+    for tile, nt in (("16", base), ("16", 2 * base), ("8", 2 * base), ("32", base)):
         monkeypatch.setenv("HYDFT_YZ_TILE", tile)
         monkeypatch.setenv("HYDFT_YZ_THREADS", str(nt))
         m = hg.Model(hg.default_params(**kw))
