@@ -124,7 +124,9 @@ __device__ __forceinline__ void store_block(cplx<R> *__restrict__ col, const cpl
     for (int r = 0; r < E; ++r) col[base + (T * (r / T) + E * (r % T)) * rs] = v[r];
 }
 
-template <typename R, int T, int E, int TX, int G, bool BAND>
+// z passes: NB ky rows (G apart) per thread, all NB columns loaded before the
+// first is transformed, so that a thread keeps NB x E loads in flight
+template <typename R, int T, int E, int TX, int G, bool BAND, int NB>
 __global__ void __launch_bounds__(TX * T * G) zinv_fast(Grid g, PassArgs<R> a, const cplx<R> *twz)
 {
     constexpr int L = T * E;
@@ -132,52 +134,61 @@ __global__ void __launch_bounds__(TX * T * G) zinv_fast(Grid g, PassArgs<R> a, c
     cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
     cplx<R> *xb = tw + 2 * L;
     const int tid = threadIdx.x, c = tid % TX, t = (tid / TX) % T, gi = tid / (TX * T);
-    const int x = blockIdx.x * TX + c, kyc = blockIdx.y * G + gi, f = blockIdx.z;
-    const bool valid = x < g.nkxc && kyc < g.nkyc;
+    const int x = blockIdx.x * TX + c, f = blockIdx.z;
     const int op = a.op[f];
     for (int i = tid; i < 2 * L; i += blockDim.x) tw[i] = twz[i];
-    const int my = valid ? signed_idx(kyc, g.My) : 0;
-    const R kx = R(x * g.kx0), ky = R(my * g.ky0);
+    const R kx = R(x * g.kx0);
     const R kz0 = R(g.kz0), kzt = R(t) * kz0;
     // kz runs over the compact band: element stride nkyc * pkx
     const int rs = g.nkyc * g.pkx;
-    const size_t col = (size_t)kyc * g.pkx + x;
-    cplx<R> v[E];
-    load_band<R, T, E, BAND>(v, a.in[f] + col, rs, t, g.Mz, g.nkzc, valid);
-    // the operator is uniform over the block
-    switch (op) {
-    case OP_ZK0:
-        if (x == 0 && my == 0 && t == 0) v[0] = cplx<R>{R(0), R(0)};
-        break;
-    case OP_IKX:
+    cplx<R> v[NB][E];
 #pragma unroll
-        for (int e = 0; e < E; ++e)
-            if (!(BAND && band_none<T, E>(e))) v[e] = ik_times(kx, v[e]);
-        break;
-    case OP_IKY:
-#pragma unroll
-        for (int e = 0; e < E; ++e)
-            if (!(BAND && band_none<T, E>(e))) v[e] = ik_times(ky, v[e]);
-        break;
-    case OP_IKZ:
-#pragma unroll
-        for (int e = 0; e < E; ++e)
-            if (!(BAND && band_none<T, E>(e))) v[e] = ik_times(band_k<R, T, E, BAND>(e, t, kz0, kzt), v[e]);
-        break;
-    case OP_NK2:
-#pragma unroll
-        for (int e = 0; e < E; ++e) {
-            if (BAND && band_none<T, E>(e)) continue;
-            const R kz = band_k<R, T, E, BAND>(e, t, kz0, kzt);
-            v[e] = R(-(kx * kx + ky * ky + kz * kz)) * v[e];
-        }
-        break;
-    default: break;
+    for (int b = 0; b < NB; ++b) {
+        const int kyc = (blockIdx.y * NB + b) * G + gi;
+        const bool valid = x < g.nkxc && kyc < g.nkyc;
+        load_band<R, T, E, BAND>(v[b], a.in[f] + (size_t)kyc * g.pkx + x, rs, t, g.Mz, g.nkzc, valid);
     }
-    __syncthreads();
-    stride_to_block<T, E, +1, R, BarBlock, TX>(v, t, xb + gi * (L + L / T) * TX + c, tw);
-    // z runs over the full axis: element stride nkyc * pkx in the ZI layout
-    if (valid) store_block<R, T, E>(a.out[f] + col, v, rs, t);
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+        const int kyc = (blockIdx.y * NB + b) * G + gi;
+        const bool valid = x < g.nkxc && kyc < g.nkyc;
+        const int my = valid ? signed_idx(kyc, g.My) : 0;
+        const R ky = R(my * g.ky0);
+        // the operator is uniform over the block
+        switch (op) {
+        case OP_ZK0:
+            if (x == 0 && my == 0 && t == 0) v[b][0] = cplx<R>{R(0), R(0)};
+            break;
+        case OP_IKX:
+#pragma unroll
+            for (int e = 0; e < E; ++e)
+                if (!(BAND && band_none<T, E>(e))) v[b][e] = ik_times(kx, v[b][e]);
+            break;
+        case OP_IKY:
+#pragma unroll
+            for (int e = 0; e < E; ++e)
+                if (!(BAND && band_none<T, E>(e))) v[b][e] = ik_times(ky, v[b][e]);
+            break;
+        case OP_IKZ:
+#pragma unroll
+            for (int e = 0; e < E; ++e)
+                if (!(BAND && band_none<T, E>(e))) v[b][e] = ik_times(band_k<R, T, E, BAND>(e, t, kz0, kzt), v[b][e]);
+            break;
+        case OP_NK2:
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                if (BAND && band_none<T, E>(e)) continue;
+                const R kz = band_k<R, T, E, BAND>(e, t, kz0, kzt);
+                v[b][e] = R(-(kx * kx + ky * ky + kz * kz)) * v[b][e];
+            }
+            break;
+        default: break;
+        }
+        if (b == 0) __syncthreads();   // the twiddles (later rows: the exchange's own barriers)
+        stride_to_block<T, E, +1, R, BarBlock, TX>(v[b], t, xb + gi * (L + L / T) * TX + c, tw);
+        // z runs over the full axis: element stride nkyc * pkx in the ZI layout
+        if (valid) store_block<R, T, E>(a.out[f] + (size_t)kyc * g.pkx + x, v[b], rs, t);
+    }
 }
 
 template <typename R, int T, int E, int TX, int G, bool BAND>
@@ -224,7 +235,7 @@ __global__ void __launch_bounds__(TX * T * G) yfwd_fast(Grid g, PassArgs<R> a, c
     if (valid) store_band<R, T, E, BAND>(a.out[f] + (size_t)z * g.nkyc * g.pkx + x, v, g.pkx, t, g.My, g.nkyc, R(1));
 }
 
-template <typename R, int T, int E, int TX, int G, bool BAND>
+template <typename R, int T, int E, int TX, int G, bool BAND, int NB>
 __global__ void __launch_bounds__(TX * T * G) zfwd_fast(Grid g, PassArgs<R> a, const cplx<R> *twz, R norm)
 {
     constexpr int L = T * E;
@@ -232,16 +243,24 @@ __global__ void __launch_bounds__(TX * T * G) zfwd_fast(Grid g, PassArgs<R> a, c
     cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
     cplx<R> *xb = tw + 2 * L;
     const int tid = threadIdx.x, c = tid % TX, t = (tid / TX) % T, gi = tid / (TX * T);
-    const int x = blockIdx.x * TX + c, kyc = blockIdx.y * G + gi, f = blockIdx.z;
-    const bool valid = x < g.nkxc && kyc < g.nkyc;
+    const int x = blockIdx.x * TX + c, f = blockIdx.z;
     for (int i = tid; i < 2 * L; i += blockDim.x) tw[i] = twz[i];
     const int rs = g.nkyc * g.pkx;
-    const size_t col = (size_t)kyc * g.pkx + x;
-    cplx<R> v[E];
-    load_block<R, T, E>(v, a.in[f] + col, rs, t, valid);
-    __syncthreads();
-    block_to_stride<T, E, -1, R, BarBlock, TX>(v, t, xb + gi * (L + L / T) * TX + c, tw);
-    if (valid) store_band<R, T, E, BAND>(a.out[f] + col, v, rs, t, g.Mz, g.nkzc, norm);
+    cplx<R> v[NB][E];
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+        const int kyc = (blockIdx.y * NB + b) * G + gi;
+        const bool valid = x < g.nkxc && kyc < g.nkyc;
+        load_block<R, T, E>(v[b], a.in[f] + (size_t)kyc * g.pkx + x, rs, t, valid);
+    }
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+        const int kyc = (blockIdx.y * NB + b) * G + gi;
+        const bool valid = x < g.nkxc && kyc < g.nkyc;
+        if (b == 0) __syncthreads();   // the twiddles (later rows: the exchange's own barriers)
+        block_to_stride<T, E, -1, R, BarBlock, TX>(v[b], t, xb + gi * (L + L / T) * TX + c, tw);
+        if (valid) store_band<R, T, E, BAND>(a.out[f] + (size_t)kyc * g.pkx + x, v[b], rs, t, g.Mz, g.nkzc, norm);
+    }
 }
 
 // smem bytes of a y/z fast pass

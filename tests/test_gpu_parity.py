@@ -368,3 +368,25 @@ def test_wide_yz_blocks_give_identical_results(hg, monkeypatch, prec, base):
     for other in out[1:]:
         for x, y in zip(out[0], other):
             assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_z_pass_row_pairs_give_identical_results(hg, monkeypatch, prec):
+    """The z passes can transform two ky rows per thread (both columns loaded
+    before the first is transformed; the inverse pass does by default, the
+    forward one with HYDFT_ZNB_FWD=2); the fields equal those of one row per
+    thread in both passes to the bit."""
+    kw = dict(ION, nx=64, ny=32, nz=48, lx=32.0, ly=16.0, lz=24.0, closure="maxwell", tau_model="constant",
+              tau=1.5, dt=0.01, gpu_precision=prec)
+    out = []
+    for flag in ("1", "2"):
+        monkeypatch.setenv("HYDFT_ZNB", flag)
+        monkeypatch.setenv("HYDFT_ZNB_FWD", flag)
+        m = hg.Model(hg.default_params(**kw))
+        n, mom, pi = seeded_state(m)
+        m.set_state(n, mom, pi)
+        m.advance(3)
+        out.append(m.get_state())
+        m.close()
+    for x, y in zip(out[0], out[1]):
+        assert np.array_equal(x, y)
