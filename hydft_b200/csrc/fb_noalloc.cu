@@ -17,12 +17,19 @@
 // tables for its own n and rmax before transforming, so calls do not depend
 // on one another's contents; two calls whose work overlaps on the GPU (on
 // different streams, or from different host threads) share the array and
-// race.  The first call on a device looks up the array's device address
-// (cudaGetSymbolAddress) and sets the transform kernel's shared-memory
-// limit; make that first call before any stream capture.
+// race.  The input and output arrays must not overlap: every block reads
+// the whole input while other blocks write their outputs.
+//
+// Every call looks up the array's device address in the current context
+// (cudaGetSymbolAddress, which allocates nothing) and sets the transform
+// kernel's shared-memory limit, so a reset device or a new context never
+// sees a stale address.  The first call on a device also loads the
+// library's kernels into that context; make that first call before any
+// stream capture.  A NULL stream is the calling thread's per-thread default
+// stream (the library is compiled with --default-stream per-thread).
 #include <cuda_runtime.h>
 
-#include <mutex>
+#include <cstdint>
 #include <string>
 
 #include "../../include/hydft_gpu.h"
@@ -39,10 +46,6 @@ constexpr size_t FB_SCRATCH = 2 * ((size_t)FB_MAX_N + 1) + 2 * (size_t)FB_MAX_N;
 // the transform's scratch: sine table, then the input weights, then the
 // output weights
 static __device__ __align__(256) double fb_scratch[FB_SCRATCH];
-
-constexpr int MAX_DEVICES = 64;
-double *g_scratch[MAX_DEVICES] = {nullptr};
-std::mutex g_mutex;
 
 // sin(pi m/(n+1)) for m < 2(n+1); the weights of direction 0 (r2k: r_j in,
 // 2 pi dr/k_j out) or 1 (k2r: k_j in, dk/(4 pi^2 r_j) out)
@@ -89,15 +92,10 @@ __global__ void fb_dst_kernel(const double *__restrict__ x, double *__restrict__
     out[k] = post[k] * 2.0 * (acc0 + acc1);
 }
 
-// once per device, with that device current: the scratch array's device
-// address and the shared-memory limit of the transform kernel
-int setup_device(int dev, double **ptr)
+// with the device current: the scratch array's device address in the
+// current context and the shared-memory limit of the transform kernel
+int setup_context(double **ptr)
 {
-    std::lock_guard<std::mutex> lock(g_mutex);
-    if (g_scratch[dev]) {
-        *ptr = g_scratch[dev];
-        return HYDFT_OK;
-    }
     void *p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, fb_scratch);
     if (e != cudaSuccess || !p) {
@@ -110,8 +108,7 @@ int setup_device(int dev, double **ptr)
         hydft::set_thread_error(std::string("fourier_bessel_noalloc: cudaFuncSetAttribute: ") + cudaGetErrorString(e));
         return HYDFT_ERR_CUDA;
     }
-    g_scratch[dev] = static_cast<double *>(p);
-    *ptr = g_scratch[dev];
+    *ptr = static_cast<double *>(p);
     return HYDFT_OK;
 }
 
@@ -129,14 +126,20 @@ extern "C" int hydft_gpu_fourier_bessel_noalloc(const double *d_in, double *d_ou
                                 std::to_string(FB_MAX_N) + ", the size of the fixed scratch array");
         return HYDFT_ERR_BAD_ARG;
     }
+    const uintptr_t a0 = reinterpret_cast<uintptr_t>(d_in), b0 = reinterpret_cast<uintptr_t>(d_out);
+    const uintptr_t bytes = sizeof(double) * (uintptr_t)n;
+    if (a0 < b0 + bytes && b0 < a0 + bytes) {
+        hydft::set_thread_error("fourier_bessel_noalloc: the input and output arrays overlap");
+        return HYDFT_ERR_BAD_ARG;
+    }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) {
+    if (e != cudaSuccess) {
         hydft::set_thread_error("fourier_bessel_noalloc: no usable current CUDA device");
         return HYDFT_ERR_CUDA;
     }
     double *scr = nullptr;
-    if (int rc = setup_device(dev, &scr)) return rc;
+    if (int rc = setup_context(&scr)) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int M = 2 * (n + 1);
     fb_tables_kernel<<<(M + 255) / 256, 256, 0, st>>>(scr, n, rmax, direction);

@@ -412,13 +412,18 @@ int gpu_fourier_bessel(int device, const double *fin, double *fout, int n, doubl
             rc = 2;
             break;
         }
-        cudaMemcpy(dx, fin, sizeof(double) * n, cudaMemcpyHostToDevice);
-        cudaMemcpy(dpre, pre.data(), sizeof(double) * n, cudaMemcpyHostToDevice);
-        cudaMemcpy(dpost, post.data(), sizeof(double) * n, cudaMemcpyHostToDevice);
-        cudaMemcpy(dsn, sn.data(), sizeof(double) * sn.size(), cudaMemcpyHostToDevice);
-        cudaFuncSetAttribute(dst_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smd, 48 * 1024));
-        dst_kernel<<<(n + 127) / 128, 128, smd>>>(dx, dpre, dpost, dout, n, dsn);
-        cudaError_t e = cudaMemcpy(fout, dout, sizeof(double) * n, cudaMemcpyDeviceToHost);
+        cudaError_t e = cudaMemcpy(dx, fin, sizeof(double) * n, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(dpre, pre.data(), sizeof(double) * n, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(dpost, post.data(), sizeof(double) * n, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(dsn, sn.data(), sizeof(double) * sn.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(dst_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)std::max<size_t>(smd, 48 * 1024));
+        if (e == cudaSuccess) {
+            dst_kernel<<<(n + 127) / 128, 128, smd>>>(dx, dpre, dpost, dout, n, dsn);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaMemcpy(fout, dout, sizeof(double) * n, cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) {
             err = std::string("fourier_bessel: ") + cudaGetErrorString(e);
             rc = 7;

@@ -229,13 +229,16 @@ int hydft_gpu_fourier_bessel(const double *f_in, double *f_out, int n, double rm
  * sine table and weights live in a fixed scratch array inside the library
  * (2(n+1) + 2n doubles for n <= HYDFT_FB_NOALLOC_MAX_N, 262 160 bytes,
  * resident on every GPU that loads the library until the process exits).
- * n above the maximum is rejected with HYDFT_ERR_BAD_ARG.  The kernels run
- * on `stream` (a cudaStream_t; NULL for the default stream) and the call
- * returns without waiting for them.  Every call rebuilds the tables for its
- * own n and rmax; calls whose work overlaps on the GPU share the scratch
- * array and race.  The first call on a device looks up the scratch array's
- * address and configures the kernel; make it before any stream capture.
- * Errors: hydft_gpu_create_error().
+ * n above the maximum is rejected with HYDFT_ERR_BAD_ARG, and so are d_in
+ * and d_out ranges that overlap (the transform reads all of d_in while it
+ * writes d_out).  The kernels run on `stream` (a cudaStream_t; NULL is the
+ * calling thread's per-thread default stream, since the library is built
+ * with --default-stream per-thread) and the call returns without waiting
+ * for them.  Every call rebuilds the tables for its own n and rmax; calls
+ * whose work overlaps on the GPU share the scratch array and race.  Every
+ * call looks up the scratch array's address in the current context; the
+ * first call on a device also loads the library's kernels there, so make
+ * it before any stream capture.  Errors: hydft_gpu_create_error().
  */
 #define HYDFT_FB_NOALLOC_MAX_N 8192
 int hydft_gpu_fourier_bessel_noalloc(const double *d_in, double *d_out, int n, double rmax,

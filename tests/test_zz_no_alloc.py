@@ -59,6 +59,41 @@ def test_noalloc_matches_allocating_entry_point_twice():
         assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
 
 
+def test_noalloc_at_the_maximum_size_then_a_smaller_one():
+    import torch
+    L = _lib()
+    # n = 8192 fills the scratch array exactly and needs the largest shared
+    # sine table; the smaller call after it must not see the larger call's
+    # leftover tables
+    nmax = 8192
+    rmax = 80.0
+    r = rmax / (nmax + 1) * np.arange(1, nmax + 1)
+    fa = np.exp(-0.5 * r) * np.sin(0.7 * r) / (1.0 + r)
+    nb, rmaxb = 1024, 30.0
+    kb = np.pi / rmaxb * np.arange(1, nb + 1)
+    fb = np.exp(-0.1 * kb * kb)
+    for f, rm, direction in ((fa, rmax, 0), (fb, rmaxb, 1), (fa, rmax, 1)):
+        ref = _allocating(f, rm, direction)
+        got = _noalloc(L, torch, f, rm, direction)
+        assert np.all(np.isfinite(got))
+        assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_noalloc_rejects_overlapping_arrays():
+    import torch
+    L = _lib()
+    n = 256
+    dev = torch.zeros(2 * n, dtype=torch.float64, device="cuda")
+    for off in (0, 1, n - 1):
+        rc = L.hydft_gpu_fourier_bessel_noalloc(dev.data_ptr(), dev.data_ptr() + 8 * off, n, 60.0, 0, None)
+        assert rc == 1
+        assert b"overlap" in L.hydft_gpu_create_error()
+    # adjacent, not overlapping: accepted
+    rc = L.hydft_gpu_fourier_bessel_noalloc(dev.data_ptr(), dev.data_ptr() + 8 * n, n, 60.0, 0, None)
+    assert rc == 0, L.hydft_gpu_create_error()
+    torch.cuda.synchronize()
+
+
 def test_noalloc_rejects_sizes_beyond_the_scratch():
     import torch
     L = _lib()
