@@ -210,88 +210,300 @@ void orc_fft1_c(int n, orc_cplx *data, int sign)
 }
 
 /* ---------------------------------------------------------------- 3-D */
+/*
+ * The 3-D transforms run the same Stockham passes (same factor order, same
+ * twiddle values, same butterflies) on OB lines at once: a batch holds
+ * element e of lane b at [e*OB + b], real and imaginary parts in separate
+ * arrays, so every butterfly is a short loop over the lanes.  Lengths with
+ * a prime factor above 64 (Bluestein) go line by line through exec_buf.
+ */
+#define OB 8
+
+typedef struct {
+    int n, nf, batched;
+    int f[64], ns[64];
+    double *twr[64], *twi[64];   /* pass s: W_n^{k r tw_step} at [k*(R-1) + r-1] */
+    double *wr, *wi;             /* W_n^t = exp(-2 pi i t/n) */
+    orc_fft1 *line;
+} bplan;
+
+static bplan *bplan_create(int n)
+{
+    bplan *p = (bplan *)calloc(1, sizeof(*p));
+    p->n = n;
+    p->line = orc_fft1_create(n);
+    if (n <= 1 || p->line->sub) return p;
+    p->batched = 1;
+    p->nf = p->line->nf;
+    p->wr = (double *)malloc(sizeof(double) * n);
+    p->wi = (double *)malloc(sizeof(double) * n);
+    for (int t = 0; t < n; ++t) {
+        p->wr[t] = creal(p->line->w[t]);
+        p->wi[t] = cimag(p->line->w[t]);
+    }
+    int Ns = 1;
+    for (int s = 0; s < p->nf; ++s) {
+        const int R = p->line->f[s];
+        p->f[s] = R;
+        p->ns[s] = Ns;
+        const int tw_step = n / (Ns * R);
+        p->twr[s] = (double *)malloc(sizeof(double) * (size_t)Ns * (R - 1) + 8);
+        p->twi[s] = (double *)malloc(sizeof(double) * (size_t)Ns * (R - 1) + 8);
+        for (int k = 0; k < Ns; ++k)
+            for (int r = 1; r < R; ++r) {
+                const long t = ((long)k * r * tw_step) % n;
+                p->twr[s][(long)k * (R - 1) + r - 1] = p->wr[t];
+                p->twi[s][(long)k * (R - 1) + r - 1] = p->wi[t];
+            }
+        Ns *= R;
+    }
+    return p;
+}
+
+static void bplan_destroy(bplan *p)
+{
+    if (!p) return;
+    for (int s = 0; s < p->nf; ++s) { free(p->twr[s]); free(p->twi[s]); }
+    free(p->wr);
+    free(p->wi);
+    orc_fft1_destroy(p->line);
+    free(p);
+}
+
+/* one batched pass of radix R; the arithmetic of each lane is that of pass():
+ * input element j + r m (j = jj Ns + k) times W^{k r tw_step}, an R-point
+ * butterfly, output element jj Ns R + k + q Ns */
+static void bpass(const bplan *p, int s, const double *restrict ar, const double *restrict ai,
+                  double *restrict br, double *restrict bi, int sign)
+{
+    const int n = p->n, R = p->f[s], Ns = p->ns[s], m = n / R;
+    const double *twr = p->twr[s], *twi = p->twi[s];
+    const double sg = sign < 0 ? 1.0 : -1.0;      /* backward: conjugate twiddles */
+    const int nj = m / Ns;
+    if (R == 4) {
+        for (int jj = 0; jj < nj; ++jj)
+            for (int k = 0; k < Ns; ++k) {
+                const long j = (long)jj * Ns + k;
+                const long d = (long)jj * Ns * 4 + k;
+                const double c1 = twr[3 * k], s1 = sg * twi[3 * k];
+                const double c2 = twr[3 * k + 1], s2 = sg * twi[3 * k + 1];
+                const double c3 = twr[3 * k + 2], s3 = sg * twi[3 * k + 2];
+                const double *x0r = ar + j * OB, *x0i = ai + j * OB;
+                const double *x1r = ar + (j + m) * OB, *x1i = ai + (j + m) * OB;
+                const double *x2r = ar + (j + 2 * m) * OB, *x2i = ai + (j + 2 * m) * OB;
+                const double *x3r = ar + (j + 3 * m) * OB, *x3i = ai + (j + 3 * m) * OB;
+                double *o0r = br + d * OB, *o0i = bi + d * OB;
+                double *o1r = br + (d + Ns) * OB, *o1i = bi + (d + Ns) * OB;
+                double *o2r = br + (d + 2 * Ns) * OB, *o2i = bi + (d + 2 * Ns) * OB;
+                double *o3r = br + (d + 3 * Ns) * OB, *o3i = bi + (d + 3 * Ns) * OB;
+                for (int b = 0; b < OB; ++b) {
+                    const double v0r = x0r[b], v0i = x0i[b];
+                    const double v1r = x1r[b] * c1 - x1i[b] * s1, v1i = x1r[b] * s1 + x1i[b] * c1;
+                    const double v2r = x2r[b] * c2 - x2i[b] * s2, v2i = x2r[b] * s2 + x2i[b] * c2;
+                    const double v3r = x3r[b] * c3 - x3i[b] * s3, v3i = x3r[b] * s3 + x3i[b] * c3;
+                    const double a0r = v0r + v2r, a0i = v0i + v2i;
+                    const double a1r = v0r - v2r, a1i = v0i - v2i;
+                    const double b0r = v1r + v3r, b0i = v1i + v3i;
+                    const double b1r = v1r - v3r, b1i = v1i - v3i;
+                    /* forward: -i b1; backward: +i b1 */
+                    const double jr = sign < 0 ? b1i : -b1i, ji = sign < 0 ? -b1r : b1r;
+                    o0r[b] = a0r + b0r; o0i[b] = a0i + b0i;
+                    o1r[b] = a1r + jr;  o1i[b] = a1i + ji;
+                    o2r[b] = a0r - b0r; o2i[b] = a0i - b0i;
+                    o3r[b] = a1r - jr;  o3i[b] = a1i - ji;
+                }
+            }
+        return;
+    }
+    if (R == 2) {
+        for (int jj = 0; jj < nj; ++jj)
+            for (int k = 0; k < Ns; ++k) {
+                const long j = (long)jj * Ns + k;
+                const long d = (long)jj * Ns * 2 + k;
+                const double c1 = twr[k], s1 = sg * twi[k];
+                const double *x0r = ar + j * OB, *x0i = ai + j * OB;
+                const double *x1r = ar + (j + m) * OB, *x1i = ai + (j + m) * OB;
+                double *o0r = br + d * OB, *o0i = bi + d * OB;
+                double *o1r = br + (d + Ns) * OB, *o1i = bi + (d + Ns) * OB;
+                for (int b = 0; b < OB; ++b) {
+                    const double v1r = x1r[b] * c1 - x1i[b] * s1, v1i = x1r[b] * s1 + x1i[b] * c1;
+                    o0r[b] = x0r[b] + v1r; o0i[b] = x0i[b] + v1i;
+                    o1r[b] = x0r[b] - v1r; o1i[b] = x0i[b] - v1i;
+                }
+            }
+        return;
+    }
+    /* direct R-point DFT, R prime (3, 5 or larger) */
+    double vr[64][OB], vi[64][OB];
+    const int step = n / R;
+    for (int jj = 0; jj < nj; ++jj)
+        for (int k = 0; k < Ns; ++k) {
+            const long j = (long)jj * Ns + k;
+            const long d = (long)jj * Ns * R + k;
+            for (int r = 0; r < R; ++r) {
+                const double *xr = ar + (j + (long)r * m) * OB, *xi = ai + (j + (long)r * m) * OB;
+                if (r == 0) {
+                    for (int b = 0; b < OB; ++b) { vr[0][b] = xr[b]; vi[0][b] = xi[b]; }
+                } else {
+                    const double c = twr[(long)k * (R - 1) + r - 1], sn = sg * twi[(long)k * (R - 1) + r - 1];
+                    for (int b = 0; b < OB; ++b) {
+                        vr[r][b] = xr[b] * c - xi[b] * sn;
+                        vi[r][b] = xr[b] * sn + xi[b] * c;
+                    }
+                }
+            }
+            for (int q = 0; q < R; ++q) {
+                double sr[OB], si[OB];
+                for (int b = 0; b < OB; ++b) { sr[b] = 0.0; si[b] = 0.0; }
+                for (int r = 0; r < R; ++r) {
+                    const long t = ((long)r * q % R) * step;
+                    const double c = p->wr[t], sn = sg * p->wi[t];
+                    for (int b = 0; b < OB; ++b) {
+                        sr[b] = sr[b] + (vr[r][b] * c - vi[r][b] * sn);
+                        si[b] = si[b] + (vr[r][b] * sn + vi[r][b] * c);
+                    }
+                }
+                double *or_ = br + (d + (long)q * Ns) * OB, *oi = bi + (d + (long)q * Ns) * OB;
+                for (int b = 0; b < OB; ++b) { or_[b] = sr[b]; oi[b] = si[b]; }
+            }
+        }
+}
+
+/* transform OB lanes held in (re, im); (wr, wi) is scratch of the same size */
+static void bexec(const bplan *p, double *re, double *im, double *wr, double *wi, int sign)
+{
+    const int n = p->n;
+    if (n <= 1) return;
+    if (!p->batched) {
+        orc_cplx *buf = (orc_cplx *)malloc(sizeof(orc_cplx) * n);
+        orc_cplx *work = (orc_cplx *)malloc(sizeof(orc_cplx) * n);
+        for (int b = 0; b < OB; ++b) {
+            for (int e = 0; e < n; ++e) buf[e] = re[e * OB + b] + I * im[e * OB + b];
+            exec_buf(p->line, buf, work, sign);
+            for (int e = 0; e < n; ++e) { re[e * OB + b] = creal(buf[e]); im[e * OB + b] = cimag(buf[e]); }
+        }
+        free(buf);
+        free(work);
+        return;
+    }
+    double *ar = re, *ai = im, *br = wr, *bi = wi;
+    for (int s = 0; s < p->nf; ++s) {
+        bpass(p, s, ar, ai, br, bi, sign);
+        double *t = ar; ar = br; br = t;
+        t = ai; ai = bi; bi = t;
+    }
+    if (ar != re) {
+        memcpy(re, ar, sizeof(double) * (size_t)n * OB);
+        memcpy(im, ai, sizeof(double) * (size_t)n * OB);
+    }
+}
+
 struct orc_fft3 {
     int nx, ny, nz, nkx;
-    orc_fft1 *px, *py, *pz;
+    bplan *px, *py, *pz;
     double norm;
     long count;
+    orc_cplx *tmp;    /* (nkx,ny,nz) work array of the backward transform */
 };
 
 orc_fft3 *orc_fft3_create(int nx, int ny, int nz)
 {
     orc_fft3 *f = (orc_fft3 *)calloc(1, sizeof(*f));
     f->nx = nx; f->ny = ny; f->nz = nz; f->nkx = nx / 2 + 1;
-    f->px = orc_fft1_create(nx);
-    f->py = orc_fft1_create(ny);
-    f->pz = orc_fft1_create(nz);
+    f->px = bplan_create(nx);
+    f->py = bplan_create(ny);
+    f->pz = bplan_create(nz);
     f->norm = 1.0 / ((double)nx * (double)ny * (double)nz);
+    f->tmp = (orc_cplx *)malloc(sizeof(orc_cplx) * (size_t)f->nkx * ny * nz);
     return f;
 }
 
 void orc_fft3_destroy(orc_fft3 *f)
 {
     if (!f) return;
-    orc_fft1_destroy(f->px);
-    orc_fft1_destroy(f->py);
-    orc_fft1_destroy(f->pz);
+    bplan_destroy(f->px);
+    bplan_destroy(f->py);
+    bplan_destroy(f->pz);
+    free(f->tmp);
     free(f);
 }
 
 long orc_fft3_count(const orc_fft3 *f) { return f->count; }
 
-/* transform along y (axis 1) or z (axis 2) of a (nkx,ny,nz) complex array */
-static void lines_yz(orc_fft3 *f, orc_cplx *a, int axis, int sign)
+/* transform along y (axis 1) or z (axis 2) of a (nkx,ny,nz) complex array,
+ * reading src and writing dst (which may be src), OB consecutive kx at once */
+static void lines_yz(orc_fft3 *f, const orc_cplx *src, orc_cplx *dst, int axis, int sign)
 {
     const int nkx = f->nkx, ny = f->ny, nz = f->nz;
-    if ((axis == 1 && ny == 1) || (axis == 2 && nz == 1)) return;
     const int len = axis == 1 ? ny : nz;
-    const int nlines = axis == 1 ? nkx * nz : nkx * ny;
-    orc_fft1 *p = axis == 1 ? f->py : f->pz;
+    const int nblk = (nkx + OB - 1) / OB;
+    const int nother = axis == 1 ? nz : ny;
+    const long stride = axis == 1 ? nkx : (long)nkx * ny;
+    const bplan *p = axis == 1 ? f->py : f->pz;
 #pragma omp parallel
     {
-        orc_cplx *buf = (orc_cplx *)malloc(sizeof(orc_cplx) * len);
-        orc_cplx *work = (orc_cplx *)malloc(sizeof(orc_cplx) * len);
+        double *re = (double *)malloc(sizeof(double) * 4 * (size_t)len * OB);
+        double *im = re + (size_t)len * OB, *wr = im + (size_t)len * OB, *wi = wr + (size_t)len * OB;
 #pragma omp for schedule(static)
-        for (int l = 0; l < nlines; ++l) {
-            long base, stride;
-            if (axis == 1) {
-                int i = l % nkx, k = l / nkx;
-                base = i + (long)nkx * ny * k;
-                stride = nkx;
-            } else {
-                int i = l % nkx, j = l / nkx;
-                base = i + (long)nkx * j;
-                stride = (long)nkx * ny;
+        for (long t = 0; t < (long)nblk * nother; ++t) {
+            const int blk = (int)(t % nblk), o = (int)(t / nblk);
+            const int i0 = blk * OB, lanes = nkx - i0 < OB ? nkx - i0 : OB;
+            const long base = i0 + (axis == 1 ? (long)nkx * ny * o : (long)nkx * o);
+            for (int e = 0; e < len; ++e) {
+                const orc_cplx *a = src + base + e * stride;
+                for (int b = 0; b < OB; ++b) {
+                    re[e * OB + b] = b < lanes ? creal(a[b]) : 0.0;
+                    im[e * OB + b] = b < lanes ? cimag(a[b]) : 0.0;
+                }
             }
-            for (int e = 0; e < len; ++e) buf[e] = a[base + e * stride];
-            exec_buf(p, buf, work, sign);
-            for (int e = 0; e < len; ++e) a[base + e * stride] = buf[e];
+            bexec(p, re, im, wr, wi, sign);
+            for (int e = 0; e < len; ++e) {
+                orc_cplx *a = dst + base + e * stride;
+                for (int b = 0; b < lanes; ++b) a[b] = re[e * OB + b] + I * im[e * OB + b];
+            }
         }
-        free(buf);
-        free(work);
+        free(re);
     }
 }
 
 void orc_fft3_fwd(orc_fft3 *f, const double *u, orc_cplx *uhat)
 {
     const int nx = f->nx, ny = f->ny, nz = f->nz, nkx = f->nkx;
-    const int nrows = ny * nz;
+    const long nrows = (long)ny * nz;
+    /* two real rows per lane: z = x_a + i x_b, Z = DFT(z);
+     * X_a[k] = (Z[k] + conj Z[-k])/2, X_b[k] = (Z[k] - conj Z[-k])/(2i) */
+    const long nblk = (nrows + 2 * OB - 1) / (2 * OB);
 #pragma omp parallel
     {
-        orc_cplx *buf = (orc_cplx *)malloc(sizeof(orc_cplx) * nx);
-        orc_cplx *work = (orc_cplx *)malloc(sizeof(orc_cplx) * nx);
+        double *re = (double *)malloc(sizeof(double) * 4 * (size_t)nx * OB);
+        double *im = re + (size_t)nx * OB, *wr = im + (size_t)nx * OB, *wi = wr + (size_t)nx * OB;
 #pragma omp for schedule(static)
-        for (int r = 0; r < nrows; ++r) {
-            const double *row = u + (long)nx * r;
-            for (int i = 0; i < nx; ++i) buf[i] = row[i];
-            exec_buf(f->px, buf, work, -1);
-            for (int i = 0; i < nkx; ++i) uhat[(long)nkx * r + i] = buf[i];
+        for (long blk = 0; blk < nblk; ++blk) {
+            const long r0 = blk * 2 * OB;
+            for (int b = 0; b < OB; ++b) {
+                const long ra = r0 + b, rb = r0 + OB + b;
+                const double *rowa = u + nx * ra, *rowb = u + nx * rb;
+                for (int i = 0; i < nx; ++i) {
+                    re[i * OB + b] = ra < nrows ? rowa[i] : 0.0;
+                    im[i * OB + b] = rb < nrows ? rowb[i] : 0.0;
+                }
+            }
+            bexec(f->px, re, im, wr, wi, -1);
+            for (int b = 0; b < OB; ++b) {
+                const long ra = r0 + b, rb = r0 + OB + b;
+                for (int i = 0; i < nkx; ++i) {
+                    const int ni = i == 0 ? 0 : nx - i;
+                    const double zr = re[i * OB + b], zi = im[i * OB + b];
+                    const double vr = re[ni * OB + b], vi = im[ni * OB + b];
+                    if (ra < nrows) uhat[(long)nkx * ra + i] = 0.5 * (zr + vr) + I * (0.5 * (zi - vi));
+                    if (rb < nrows) uhat[(long)nkx * rb + i] = 0.5 * (zi + vi) - I * (0.5 * (zr - vr));
+                }
+            }
         }
-        free(buf);
-        free(work);
+        free(re);
     }
-    lines_yz(f, uhat, 1, -1);
-    lines_yz(f, uhat, 2, -1);
+    if (ny > 1) lines_yz(f, uhat, uhat, 1, -1);
+    if (nz > 1) lines_yz(f, uhat, uhat, 2, -1);
     const long nh = (long)nkx * ny * nz;
 #pragma omp parallel for schedule(static)
     for (long q = 0; q < nh; ++q) uhat[q] *= f->norm;
@@ -301,32 +513,52 @@ void orc_fft3_fwd(orc_fft3 *f, const double *u, orc_cplx *uhat)
 void orc_fft3_bwd(orc_fft3 *f, const orc_cplx *uhat, double *u)
 {
     const int nx = f->nx, ny = f->ny, nz = f->nz, nkx = f->nkx;
-    const long nh = (long)nkx * ny * nz;
-    orc_cplx *a = (orc_cplx *)malloc(sizeof(orc_cplx) * nh);
-    memcpy(a, uhat, sizeof(orc_cplx) * nh);
-    lines_yz(f, a, 2, +1);
-    lines_yz(f, a, 1, +1);
-    const int nrows = ny * nz;
+    const orc_cplx *src = uhat;
+    if (nz > 1) { lines_yz(f, src, f->tmp, 2, +1); src = f->tmp; }
+    if (ny > 1) { lines_yz(f, src, f->tmp, 1, +1); src = f->tmp; }
+    const long nrows = (long)ny * nz;
+    /* two half-spectrum rows per lane: Z = A + i B with A, B the Hermitian
+     * extensions of rows a and b; z = IDFT(Z) gives x_a = Re z, x_b = Im z.
+     * The imaginary parts of the self-conjugate bins (kx = 0 and kx = nx/2)
+     * are dropped, as a c2r transform ignores them. */
+    const long nblk = (nrows + 2 * OB - 1) / (2 * OB);
 #pragma omp parallel
     {
-        orc_cplx *buf = (orc_cplx *)malloc(sizeof(orc_cplx) * nx);
-        orc_cplx *work = (orc_cplx *)malloc(sizeof(orc_cplx) * nx);
+        double *re = (double *)malloc(sizeof(double) * 4 * (size_t)nx * OB);
+        double *im = re + (size_t)nx * OB, *wr = im + (size_t)nx * OB, *wi = wr + (size_t)nx * OB;
 #pragma omp for schedule(static)
-        for (int r = 0; r < nrows; ++r) {
-            const orc_cplx *h = a + (long)nkx * r;
-            /* Hermitian extension along x; the imaginary parts of the
-             * self-conjugate bins contribute only to the discarded
-             * imaginary part of the result. */
-            for (int i = 0; i < nkx; ++i) buf[i] = h[i];
-            for (int i = nkx; i < nx; ++i) buf[i] = conj(h[nx - i]);
-            exec_buf(f->px, buf, work, +1);
-            double *row = u + (long)nx * r;
-            for (int i = 0; i < nx; ++i) row[i] = creal(buf[i]);
+        for (long blk = 0; blk < nblk; ++blk) {
+            const long r0 = blk * 2 * OB;
+            for (int b = 0; b < OB; ++b) {
+                const long ra = r0 + b, rb = r0 + OB + b;
+                const orc_cplx *ha = src + (long)nkx * (ra < nrows ? ra : 0);
+                const orc_cplx *hb = src + (long)nkx * (rb < nrows ? rb : 0);
+                const double ma = ra < nrows ? 1.0 : 0.0, mb = rb < nrows ? 1.0 : 0.0;
+                for (int i = 0; i < nx; ++i) {
+                    const int h = i < nkx ? i : nx - i;
+                    const int self = (i == 0) || (2 * i == nx);
+                    double ar = ma * creal(ha[h]), ai = self ? 0.0 : ma * cimag(ha[h]);
+                    double br = mb * creal(hb[h]), bi = self ? 0.0 : mb * cimag(hb[h]);
+                    if (i >= nkx) { ai = -ai; bi = -bi; }
+                    re[i * OB + b] = ar - bi;
+                    im[i * OB + b] = ai + br;
+                }
+            }
+            bexec(f->px, re, im, wr, wi, +1);
+            for (int b = 0; b < OB; ++b) {
+                const long ra = r0 + b, rb = r0 + OB + b;
+                if (ra < nrows) {
+                    double *row = u + (long)nx * ra;
+                    for (int i = 0; i < nx; ++i) row[i] = re[i * OB + b];
+                }
+                if (rb < nrows) {
+                    double *row = u + (long)nx * rb;
+                    for (int i = 0; i < nx; ++i) row[i] = im[i * OB + b];
+                }
+            }
         }
-        free(buf);
-        free(work);
+        free(re);
     }
-    free(a);
     f->count++;
 }
 

@@ -197,6 +197,8 @@ static int min_nonpositive(const double *a, long n)
 static int tf_alpha_of_n(const term_t *t, const double *n, double *alpha, long nc)
 {
     if (min_nonpositive(n, nc)) return 10;
+    orc_fd_init();
+#pragma omp parallel for schedule(static)
     for (long q = 0; q < nc; ++q) alpha[q] = orc_fd_alpha_from_ip12(n[q] / t->cn, NULL);
     return 0;
 }
@@ -210,11 +212,13 @@ int orc_model_term_add_mu(orc_model *m, int i, const double *n, const orc_cplx *
     switch (t->id) {
     case ORC_TERM_IDEAL:   /* fe_ideal_classical.f90:33-41 */
         if (min_nonpositive(n, nc)) return 11;
+#pragma omp parallel for schedule(static)
         for (long q = 0; q < nc; ++q) mu[q] = mu[q] + log(n[q]) / t->beta;
         return 0;
     case ORC_TERM_TF: {    /* fe_kinetic_tfk.f90:74-82 */
         int rc = tf_alpha_of_n(t, n, t->alpha, nc);
         if (rc) return rc;
+#pragma omp parallel for schedule(static)
         for (long q = 0; q < nc; ++q) mu[q] = mu[q] + t->alpha[q] / t->beta;
         return 0;
     }
@@ -225,9 +229,12 @@ int orc_model_term_add_mu(orc_model *m, int i, const double *n, const orc_cplx *
             else memset(t->gn + (d - 1) * nc, 0, sizeof(double) * nc);
         }
         double *negk2 = dalloc(nh);
+#pragma omp parallel for schedule(static)
         for (long q = 0; q < nh; ++q) negk2[q] = -spc->g.k2[q];
         orc_spec_convolve(spc, negk2, nhat, t->lapn);
         free(negk2);
+        orc_fd_init();
+#pragma omp parallel for schedule(static)
         for (long q = 0; q < nc; ++q) {
             double a = orc_fd_alpha_from_ip12(n[q] / t->cn, NULL);
             double xi = orc_fd_xi(a);
@@ -240,6 +247,7 @@ int orc_model_term_add_mu(orc_model *m, int i, const double *n, const orc_cplx *
     }
     case ORC_TERM_HARTREE:  /* fe_hartree.f90:46-54 */
         orc_spec_convolve(spc, t->vk, nhat, t->w);
+#pragma omp parallel for schedule(static)
         for (long q = 0; q < nc; ++q) mu[q] = mu[q] + t->w[q];
         return 0;
     case ORC_TERM_RY: {     /* fe_correlation_ry.f90:64-80 */
@@ -248,6 +256,7 @@ int orc_model_term_add_mu(orc_model *m, int i, const double *n, const orc_cplx *
         b[0] = nhat[0] - t->n0;
         orc_spec_convolve(spc, t->ck, b, t->w);
         free(b);
+#pragma omp parallel for schedule(static)
         for (long q = 0; q < nc; ++q) mu[q] = mu[q] - t->w[q] / t->beta;
         return 0;
     }
@@ -259,6 +268,7 @@ int orc_model_term_add_mu(orc_model *m, int i, const double *n, const orc_cplx *
 int orc_model_mu_total(orc_model *m, const double *n, const orc_cplx *nhat, double *mu)
 {
     const long nc = NC(m);
+#pragma omp parallel for schedule(static)
     for (long q = 0; q < nc; ++q) mu[q] = 0.0;
     for (int i = 0; i < m->nterms; ++i) {
         int rc = orc_model_term_add_mu(m, i, n, nhat, mu);
@@ -354,6 +364,7 @@ static void vext_eval(orc_model *m, double t)
                     m->ext_v[q] = -a * exp(-0.5 * r2 / (m->ext_width * m->ext_width));
                 }
         orc_spec_grad(&m->spc, m->ext_v, m->ext_f);
+#pragma omp parallel for schedule(static)
         for (long q = 0; q < 3 * nc; ++q) m->ext_f[q] = -m->ext_f[q];
     }
 }
@@ -638,6 +649,7 @@ void orc_model_velocity(orc_model *m)
 {
     const long nc = NC(m);
     for (int d = 0; d < 3; ++d)
+#pragma omp parallel for schedule(static)
         for (long q = 0; q < nc; ++q) m->u[d * nc + q] = m->mom[d * nc + q] / (m->mass * m->n[q]);
 }
 
@@ -652,6 +664,7 @@ int orc_model_rhs(orc_model *m, double t, double *dn, double *dmom, double *dpi)
     orc_spec_fwd(spc, m->n, m->nhat);
     /* continuity */
     orc_spec_div(spc, m->mom, dn);
+#pragma omp parallel for schedule(static)
     for (long q = 0; q < nc; ++q) dn[q] = -dn[q] / m->mass;
     /* chemical potential and its gradient */
     int rc = orc_model_mu_total(m, m->n, m->nhat, m->mu);
@@ -671,13 +684,17 @@ int orc_model_rhs(orc_model *m, double t, double *dn, double *dmom, double *dpi)
             continue;
         }
         for (int j = 1; j <= 3; ++j)
+#pragma omp parallel for schedule(static)
             for (long q = 0; q < nc; ++q)
                 m->flux[(j - 1) * nc + q] = m->mom[(i - 1) * nc + q] * m->u[(j - 1) * nc + q];
         orc_spec_div(spc, m->flux, m->divf);
+#pragma omp parallel for schedule(static)
         for (long q = 0; q < nc; ++q) m->divf[q] = m->divf[q] + m->n[q] * m->gmu[(i - 1) * nc + q];
         double mean = orc_spec_mean(spc, m->divf);
+#pragma omp parallel for schedule(static)
         for (long q = 0; q < nc; ++q) dm[q] = -(m->divf[q] - mean) + m->fpi[(i - 1) * nc + q];
         if (m->ext_active)
+#pragma omp parallel for schedule(static)
             for (long q = 0; q < nc; ++q) dm[q] = dm[q] + m->n[q] * m->ext_f[(i - 1) * nc + q];
     }
     /* stress advection */
@@ -685,8 +702,10 @@ int orc_model_rhs(orc_model *m, double t, double *dn, double *dmom, double *dpi)
         for (int c = 0; c < 6; ++c) {
             orc_spec_grad(spc, m->pi + c * nc, m->gpi);
             double *dp = dpi + c * nc;
+#pragma omp parallel for schedule(static)
             for (long q = 0; q < nc; ++q) dp[q] = 0.0;
             for (int d = 0; d < ndim; ++d)
+#pragma omp parallel for schedule(static)
                 for (long q = 0; q < nc; ++q) dp[q] = dp[q] - m->u[d * nc + q] * m->gpi[d * nc + q];
         }
     }
@@ -751,15 +770,21 @@ int orc_model_advance(orc_model *m)
         if (m->evolve) stress_pi0(m, m->u, m->pi0_old);
         const double dt = m->dt;
         if (s == 0) {
+#pragma omp parallel for schedule(static)
             for (long q = 0; q < nc; ++q) m->n[q] = m->n[q] + dt * RK_A[0] * m->dn[q];
+#pragma omp parallel for schedule(static)
             for (long q = 0; q < 3 * nc; ++q) m->mom[q] = m->mom[q] + dt * RK_A[0] * m->dmom[q];
             if (m->evolve)
+#pragma omp parallel for schedule(static)
                 for (long q = 0; q < 6 * nc; ++q) m->pi[q] = m->pi[q] + dt * RK_A[0] * m->dpi[q];
         } else {
+#pragma omp parallel for schedule(static)
             for (long q = 0; q < nc; ++q) m->n[q] = m->n[q] + dt * (RK_A[s] * m->dn[q] + RK_B[s] * m->dn_o[q]);
+#pragma omp parallel for schedule(static)
             for (long q = 0; q < 3 * nc; ++q)
                 m->mom[q] = m->mom[q] + dt * (RK_A[s] * m->dmom[q] + RK_B[s] * m->dmom_o[q]);
             if (m->evolve)
+#pragma omp parallel for schedule(static)
                 for (long q = 0; q < 6 * nc; ++q)
                     m->pi[q] = m->pi[q] + dt * (RK_A[s] * m->dpi[q] + RK_B[s] * m->dpi_o[q]);
         }
@@ -773,6 +798,7 @@ int orc_model_advance(orc_model *m)
             stress_pi0(m, m->u, m->pi0);
             double fac = exp(-dts / m->s_tau);
             double phi = (m->s_tau / dts) * (1.0 - fac);
+#pragma omp parallel for schedule(static)
             for (long q = 0; q < 6 * nc; ++q)
                 m->pi[q] = m->pi0[q] - (m->pi0[q] - m->pi0_old[q]) * phi + (m->pi[q] - m->pi0_old[q]) * fac;
             for (int c = 0; c < 6; ++c) orc_spec_dealias(spc, m->pi + c * nc);

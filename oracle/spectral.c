@@ -116,6 +116,7 @@ void orc_spec_bwd(orc_spec *s, const orc_cplx *uhat, double *u) { orc_fft3_bwd(s
 void orc_spec_grad_hat(orc_spec *s, const orc_cplx *uhat, int idir, double *du)
 {
     const orc_grid *g = &s->g;
+#pragma omp parallel for schedule(static) collapse(2)
     for (int k = 0; k < g->nz; ++k)
         for (int j = 0; j < g->ny; ++j)
             for (int i = 0; i < g->nkx; ++i) {
@@ -144,6 +145,7 @@ void orc_spec_lap(orc_spec *s, const double *u, double *lu)
 {
     orc_fft3_fwd(s->fft, u, s->w2);
     const long nh = nhalf(s);
+#pragma omp parallel for schedule(static)
     for (long q = 0; q < nh; ++q) s->w2[q] = -s->g.k2[q] * s->w2[q] * s->g.mask[q];
     orc_fft3_bwd(s->fft, s->w2, lu);
 }
@@ -153,9 +155,11 @@ void orc_spec_div(orc_spec *s, const double *v, double *dv)
 {
     const orc_grid *g = &s->g;
     const long nh = nhalf(s), nc = ncell(s);
+#pragma omp parallel for schedule(static)
     for (long q = 0; q < nh; ++q) s->w1[q] = 0;
     for (int d = 1; d <= g->ndim; ++d) {
         orc_fft3_fwd(s->fft, v + (d - 1) * nc, s->w2);
+#pragma omp parallel for schedule(static) collapse(2)
         for (int k = 0; k < g->nz; ++k)
             for (int j = 0; j < g->ny; ++j)
                 for (int i = 0; i < g->nkx; ++i) {
@@ -164,6 +168,7 @@ void orc_spec_div(orc_spec *s, const double *v, double *dv)
                     s->w1[q] = s->w1[q] + I * kd * s->w2[q];
                 }
     }
+#pragma omp parallel for schedule(static)
     for (long q = 0; q < nh; ++q) s->w1[q] *= g->mask[q];
     orc_fft3_bwd(s->fft, s->w1, dv);
 }
@@ -172,6 +177,7 @@ void orc_spec_div(orc_spec *s, const double *v, double *dv)
 void orc_spec_convolve(orc_spec *s, const double *kern, const orc_cplx *uhat, double *cu)
 {
     const long nh = nhalf(s);
+#pragma omp parallel for schedule(static)
     for (long q = 0; q < nh; ++q) s->w1[q] = kern[q] * uhat[q] * s->g.mask[q];
     orc_fft3_bwd(s->fft, s->w1, cu);
 }
@@ -181,6 +187,7 @@ void orc_spec_dealias(orc_spec *s, double *u)
 {
     orc_fft3_fwd(s->fft, u, s->w2);
     const long nh = nhalf(s);
+#pragma omp parallel for schedule(static)
     for (long q = 0; q < nh; ++q) s->w2[q] *= s->g.mask[q];
     orc_fft3_bwd(s->fft, s->w2, u);
 }
