@@ -136,6 +136,7 @@ struct orc_model {
     double *ext_v, *ext_f;
     /* state and work */
     double t, dt;
+    double ts;      /* stage time of the step in progress */
     int step;
     double *n, *mom, *pi;
     double *u, *mu, *gmu, *flux, *divf;
@@ -757,14 +758,17 @@ int orc_model_compute_dt(orc_model *m)
 static const double RK_A[3] = {32.0 / 60.0, 25.0 / 60.0, 45.0 / 60.0};
 static const double RK_B[3] = {0.0, -17.0 / 60.0, -25.0 / 60.0};
 
-/* model.f90:186-227 */
-int orc_model_advance(orc_model *m)
+/* one pass of the stage loop of model.f90:186-227 (s = 0, 1, 2); stage 0
+ * starts the step at t, stage 2 finishes it */
+int orc_model_stage(orc_model *m, int s)
 {
     orc_spec *spc = &m->spc;
     const long nc = NC(m);
     const int ndim = spc->g.ndim;
-    double ts = m->t;
-    for (int s = 0; s < 3; ++s) {
+    if (s < 0 || s > 2) return 99;
+    if (s == 0) m->ts = m->t;
+    double ts = m->ts;
+    {
         int rc = orc_model_rhs(m, ts, m->dn, m->dmom, m->dpi);
         if (rc) return rc;
         if (m->evolve) stress_pi0(m, m->u, m->pi0_old);
@@ -806,8 +810,21 @@ int orc_model_advance(orc_model *m)
         orc_spec_dealias(spc, m->n);
         for (int i = 0; i < ndim; ++i) orc_spec_dealias(spc, m->mom + i * nc);
     }
-    m->t = m->t + m->dt;
-    m->step = m->step + 1;
+    m->ts = ts;
+    if (s == 2) {
+        m->t = m->t + m->dt;
+        m->step = m->step + 1;
+    }
+    return 0;
+}
+
+/* model.f90:186-227 */
+int orc_model_advance(orc_model *m)
+{
+    for (int s = 0; s < 3; ++s) {
+        int rc = orc_model_stage(m, s);
+        if (rc) return rc;
+    }
     return 0;
 }
 

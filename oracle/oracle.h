@@ -191,6 +191,8 @@ void orc_model_destroy(orc_model *m);
 int orc_model_rhs(orc_model *m, double t, double *dn, double *dmom, double *dpi);
 int orc_model_compute_dt(orc_model *m);
 int orc_model_advance(orc_model *m);
+/* stage s (0, 1, 2) of one RK3 step alone: three calls in order = advance */
+int orc_model_stage(orc_model *m, int s);
 void orc_model_velocity(orc_model *m);
 int orc_model_set_ic(orc_model *m, int kind, double amp, const int mode[3], double width);
 

@@ -96,6 +96,7 @@ def lib():
         L.orc_model_set.argtypes = [_P, C.c_char_p, _D]
         L.orc_model_rhs.argtypes = [_P, _D, _P, _P, _P]
         L.orc_model_advance.argtypes = [_P]
+        L.orc_model_stage.argtypes = [_P, _I]
         L.orc_model_compute_dt.argtypes = [_P]
         L.orc_model_ncells.argtypes = [_P]
         L.orc_model_has_pi.argtypes = [_P]
@@ -447,6 +448,13 @@ class Model:
             rc = lib().orc_model_advance(self.h)
             if rc:
                 raise RuntimeError("advance failed (%d)" % rc)
+
+    def stage(self, s):
+        """Stage s (0, 1, 2) of one RK3 step alone; stages 0, 1, 2 in order
+        are one advance()."""
+        rc = lib().orc_model_stage(self.h, int(s))
+        if rc:
+            raise RuntimeError("stage failed (%d)" % rc)
 
     def fft_count(self):
         return lib().orc_model_fft_count(self.h)
