@@ -53,44 +53,106 @@ def initial_density(n, L, n0, seed=2024):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled through NVML
+    every 10 ms while the timed region runs (nvidia-smi every 100 ms when
+    NVML is unavailable).  Reading only: no clock or device setting is
+    changed."""
 
-    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits
+    REASONS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+               "hw_thermal_slowdown": 0x40, "hw_power_brake_slowdown": 0x80}
 
-    def __init__(self, gpu_index):
-        self.gpu = gpu_index
-        self.proc = None
-        self.lines = []
+    def __init__(self, cuda_device, period=0.01):
+        self.dev = cuda_device
+        self.period = period
+        self.samples = []          # (wall time, sm MHz, max sm MHz, reasons bitmask, power W)
         self.window = None
+        self.source = None
+        self._stop = threading.Event()
+        self.thread = None
 
     def mark(self, t0, t1):
         """Keep only the samples taken between wall-clock times t0 and t1."""
         self.window = (t0, t1)
 
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.dev)
+            bus = "%08X:%02X:%02X.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+            ids = [x for x in vis.split(",") if x.strip()]
+            idx = int(ids[self.dev]) if self.dev < len(ids) and ids[self.dev].isdigit() else self.dev
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(idx)
+
+    def _run_nvml(self, nv, h):
+        smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        while not self._stop.is_set():
+            t = time.time()
+            try:
+                sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+                pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+            except Exception:
+                break
+            self.samples.append((t, sm, smax, rs, pw))
+            self._stop.wait(self.period)
+
+    def _run_smi(self, proc):
+        import datetime
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                rs = 0
+                for nm, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        rs |= self.REASONS[nm]
+                self.samples.append((ts, float(parts[1]), float(parts[2]), rs, float(parts[3])))
+            except ValueError:
+                continue
+
     def start(self):
         try:
+            nv, h = self._nvml_handle()
+            self.source = "nvml, 10 ms"
+            self.thread = threading.Thread(target=self._run_nvml, args=(nv, h), daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            pass
+        fields = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                  "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                  "clocks_event_reasons.sw_power_cap")
+        try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                ["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + fields, "--format=csv,noheader,nounits",
                  "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.source = "nvidia-smi, 100 ms"
+            self.thread = threading.Thread(target=self._run_smi, args=(self.proc,), daemon=True)
             self.thread.start()
         except OSError:
-            self.proc = None
-
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.source = None
 
     def stop(self):
-        if self.proc is None:
+        self._stop.set()
+        if self.source and self.source.startswith("nvidia-smi"):
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
+        if self.source is None:
             return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
         out = self._summary(self.window)
         if out is None and self.window is not None:
             out = self._summary(None)
@@ -99,32 +161,13 @@ class ClockSampler:
         return out
 
     def _summary(self, window):
-        import datetime
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 10:
-                continue
-            if window is not None:
-                try:
-                    ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
-                except ValueError:
-                    continue
-                if not (window[0] - 0.05 <= ts <= window[1] + 0.05):
-                    continue
-            try:
-                sm.append(float(parts[2]))
-                smax.append(float(parts[3]))
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[6:10]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        if not sm:
+        sel = [s for s in self.samples if window is None or window[0] - 0.005 <= s[0] <= window[1] + 0.005]
+        if not sel:
             return None
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        reasons = sorted(nm for nm, bit in self.REASONS.items() if any(s[3] & bit for s in sel))
+        return {"sm_mhz": float(np.median([s[1] for s in sel])), "sm_max_mhz": float(max(s[2] for s in sel)),
+                "reasons": reasons, "samples": len(sel), "power_w_max": float(max(s[4] for s in sel)),
+                "source": self.source}
 
 
 def measured_peak():
@@ -150,55 +193,118 @@ def profile_traffic(kernel, precision):
     return None
 
 
-def cpu_baseline(structure, threads, steps, n=64):
-    """The FP64 oracle (reference algorithm, CPU) on a 64^3 sample of the
-    workload: same physics and resolution (L scaled with N)."""
+def workload_config(n, L, world):
+    """The workload's description, identical in both arms."""
+    return {"workload": "maxwell_ion_%d^3" % n, "grid": [n, n, n], "box_L": L,
+            "gamma": 50.0, "kappa": 2.0, "closure": "maxwell", "tau_model": "ichimaru",
+            "transport": "yukawa_fit", "hnc": "yukawa, nr 4096, rmax 80, tol 1e-9",
+            "ic": "gaussian random delta n, power ~ exp(-q^2), rms 1e-2, seed 2024; u = 0, Pi = 0",
+            "dt": "compute_dt at t = 0, cfl 0.4",
+            "parallelism": "replicas" if world > 1 else "single",
+            "l2": "inputs larger than L2 (working set ~GBs)"}
+
+
+def _oracle():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
-    L = 64.0 * n / 256.0
-    orc.set_threads(threads)
+    return orc
+
+
+def _ic_module():
+    """hydft_b200/ic.py loaded as a plain module (numpy only), so that the
+    reference arm does not import the package or load its GPU library."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("_hydft_ic", os.path.join(ROOT, "hydft_b200", "ic.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def oracle_workload_model(orc, n, L, structure):
+    """The oracle (the reference's FP64 CPU algorithm, literal transform
+    schedule) set up on the workload: structure = dict(k, c, u_ex,
+    du_dgamma) from an HNC solve."""
+    n0 = 3 / (4 * np.pi)
     p = orc.params(kind="ion", gamma=50.0, kappa=2.0, nx=n, ny=n, nz=n, lx=L, ly=L, lz=L,
-                   closure="maxwell", transport="yukawa_fit", tau_model="ichimaru", cfl=0.4)
-    st = orc.Structure(structure["k"], structure["c"], 3 / (4 * np.pi), structure["u_ex"],
-                       structure["du_dgamma"], True)
+                   closure="maxwell", transport="yukawa_fit", tau_model="ichimaru", cfl=0.4,
+                   hnc_nr=4096, hnc_rmax=80.0)
+    st = orc.Structure(structure["k"], structure["c"], n0, structure["u_ex"], structure["du_dgamma"], True)
     m = orc.Model(p, st)
-    m.set_state(initial_density(n, L, 3 / (4 * np.pi)))
+    d = _ic_module().gaussian_spectrum_field(n, n, n, L, L, L, 2024, qc=1.0)
+    m.set_state(n0 * (1.0 + 1e-2 * d))
     m.compute_dt()
-    m.advance(1)       # warm-up (plans, page faults)
+    return m
+
+
+def time_oracle_stages(m, warmup, samples):
+    """Time `samples` RK3 stages of the oracle after `warmup` stages; the
+    stages cycle 1, 2, 3, so three consecutive samples are one RK3 step.
+    Returns (seconds, stages run before the timed ones)."""
+    s = 0
+    for _ in range(warmup):
+        m.stage(s % 3)
+        s += 1
     t0 = time.perf_counter()
-    m.advance(steps)
-    el = time.perf_counter() - t0
-    return n ** 3 * steps / el, el
+    for _ in range(samples):
+        m.stage(s % 3)
+        s += 1
+    return time.perf_counter() - t0
+
+
+STAGE_SAMPLE = ("each sample is one of the three RK3 stages of the full %d^3 workload step (rhs + stage update "
+                "+ relaxation + dealias, the reference's literal 123-transform stage), stages cycling 1,2,3; "
+                "a sample counts as 1/3 cell-step per cell; FP64 oracle restatement of the reference CPU path "
+                "(model.f90:186-227), OpenMP over %d host threads (%s)")
 
 
 def run_reference(args):
+    """The reference's algorithm on the host cores: the FP64 oracle on the
+    same workload (grid, box, physics, initial state, dt) as the GPU arm,
+    with its HNC solved on the CPU too; nothing of the GPU library is
+    loaded.  Each of the K timed steps is one RK3 stage of the full grid."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return 0
-    import hydft_b200 as hg   # only for the HNC structure table of the workload
-    threads = os.cpu_count() or 1
-    try:
-        st = structure_for_workload(hg, device=0)
-    except Exception:
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import oracle as orc
-        n0 = 3 / (4 * np.pi)
-        pot = orc.make_pot("yukawa", 50.0, 2.0)
-        s = orc.structure_from_hnc(pot, n0, 4096, 80.0, 1e-9, 0.2, 20000, with_derivative=True)
-        st = dict(k=s.k, c=s.c, u_ex=s.u_ex, du_dgamma=s.du_dgamma)
-    steps = max(1, args.steps)
-    v, el = cpu_baseline(st, threads, steps, n=args.ref_n)
+    orc = _oracle()
+    threads = host_threads()
+    orc.set_threads(threads)
+    n, L = args.n, 64.0
+    t0 = time.perf_counter()
+    s = orc.structure_from_hnc(orc.make_pot("yukawa", 50.0, 2.0), 3 / (4 * np.pi), 4096, 80.0, 1e-9, 0.2,
+                               20000, with_derivative=True)
+    m = oracle_workload_model(orc, n, L, dict(k=s.k, c=s.c, u_ex=s.u_ex, du_dgamma=s.du_dgamma))
+    setup_s = time.perf_counter() - t0
+    samples = max(1, args.steps)
+    el = time_oracle_stages(m, args.warmup, samples)
+    v = float(n) ** 3 * (samples / 3.0) / el
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / steps,
+            "steps": samples, "warmup": args.warmup, "ms_per_step": 1e3 * el / samples,
+            "ms_per_rk3_step": 3e3 * el / samples,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
-            "config": {"workload": "maxwell_ion_256^3 (sampled at %d^3)" % args.ref_n, "grid": args.ref_n,
-                       "steps_per_sample": steps},
+            "data": "synthetic", "config": workload_config(n, L, world),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": "%d^3 Maxwell ions, same physics and dx (L=%g), %d RK3 steps, "
-                                       "FP64 oracle restatement of the reference CPU path, OpenMP %d threads"
-                                       % (args.ref_n, 64.0 * args.ref_n / 256, steps, threads)},
-            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                             "sample": STAGE_SAMPLE % (n, threads, cpu_model())},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "setup_s": setup_s, "dt": m.dt, "host": {"threads": threads, "cpu": cpu_model()}}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -416,14 +522,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256)
-    ap.add_argument("--ref-n", type=int, default=64)
+    ap.add_argument("--err-steps", type=int, default=2000,
+                    help="RK3 steps of the FP32-vs-FP64 field error check (the workload's 2000)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-plain leg")
     ap.add_argument("--no-cufft", action="store_true", help="skip the cuFFT comparator")
     ap.add_argument("--quick", action="store_true",
                     help="setup, warm-up and the timed steps only (for profiler captures)")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
-    ap.add_argument("--batch-members", type=int, default=0,
+    ap.add_argument("--batch-members", type=int, default=256,
                     help="also time the ensemble workload with this many members (0: skip)")
     ap.add_argument("--workload", default="maxwell256", choices=["maxwell256", "batch", "serve"],
                     help="batch: time only the ensemble workload (256 members unless --batch-members); "
@@ -533,7 +640,9 @@ def main():
     roof = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": peak_kind, "share": dms / tot,
             "bytes_per_launch": dbytes, "avg_launch_ms": dms / dn,
-            "traffic": profile_traffic(dname, "fp32")}
+            "traffic": profile_traffic(dname, "fp32"),
+            "traffic_source": "profiles/maxwell256_fp32_kernels.md (ncu dram bytes of one full-size launch, "
+                              "committed capture; not measured in this run)"}
     kernels = {k: {"ms_per_step": v[0] / 2, "launches_per_step": v[2] / 2,
                    "GBps": (v[1] / (v[0] / v[2] * 1e-3) / 1e9) if v[0] > 0 and v[1] > 0 else None}
                for k, v in prof.items()}
@@ -560,8 +669,8 @@ def main():
         m64.set_state(nin, zeros3, zeros6)
         m64.set_time(0.0, dt)
         s64 = torch.cuda.ExternalStream(m64.stream_ptr(), device=dev)
-        k64 = max(2, args.steps // 4)
-        m64.advance(1)
+        k64 = max(1, args.steps)
+        m64.advance(max(3, args.warmup))
         torch.cuda.synchronize(dev)
         f0 = torch.cuda.Event(enable_timing=True)
         f1 = torch.cuda.Event(enable_timing=True)
@@ -570,19 +679,33 @@ def main():
         f1.record(s64)
         torch.cuda.synchronize(dev)
         v64 = cells * k64 / (f0.elapsed_time(f1) * 1e-3)
-        # same number of steps from the same state for the error
+        # the workload's 2000 steps from the same initial state in FP32 and
+        # FP64 (a fresh FP64 model), then the relative l2 error per field
+        nerr = max(1, args.err_steps)
+        m64.close()
+        m64 = hg.Model(workload_params(hg, n, "fp64"), structure=st, device=dev)
+        m64.set_state(nin, zeros3, zeros6)
+        m64.set_time(0.0, dt)
         m32b = hg.Model(workload_params(hg, n, "fp32"), structure=st, device=dev)
         m32b.set_state(nin, zeros3, zeros6)
         m32b.set_time(0.0, dt)
-        m32b.advance(1 + k64)
+        t_err = time.perf_counter()
+        m64.advance(nerr)
+        m32b.advance(nerr)
         a = m32b.get_state()
         b = m64.get_state()
+        t_err = time.perf_counter() - t_err
         errs = {}
         for name, x, y in (("n", a[0], b[0]), ("mom", a[1], b[1]), ("pi", a[2], b[2])):
             errs[name] = float(np.linalg.norm(x - y) / np.linalg.norm(y))
         errs["dn"] = float(np.linalg.norm((a[0] - n0) - (b[0] - n0)) / np.linalg.norm(b[0] - n0))
-        extra["fp64_plain"] = {"value": v64, "unit": UNIT, "ratio_fp32_over_fp64": value / world / v64}
-        extra["fp32_rel_err_vs_fp64"] = dict(errs, steps=1 + k64)
+        errs["max"] = max(errs["n"], errs["mom"], errs["pi"])
+        errs["within_1e-5"] = bool(errs["max"] <= 1e-5)
+        extra["fp64_plain"] = {"value": v64, "unit": UNIT, "steps": k64, "ratio_fp32_over_fp64": value / world / v64}
+        extra["fp32_rel_err_vs_fp64"] = dict(errs, steps=nerr, t=nerr * dt, wall_s=t_err,
+                                             definition="||x32 - x64||_2 / ||x64||_2 over each field after "
+                                                        "the steps, same initial state and dt")
+        del a, b
         m64.close()
         m32b.close()
 
@@ -626,20 +749,25 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, el = cpu_baseline(st, 1, 1, n=64)
-        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": "64^3 Maxwell ions, same physics and dx (L=16), 1 RK3 step (%.1f s), "
-                         "FP64 oracle restatement of the reference serial CPU path" % el}
+        # the oracle on the same 256^3 workload, one warm-up stage and one
+        # RK3 step (three stage samples) timed, all host threads
+        orc = _oracle()
+        threads = host_threads()
+        orc.set_threads(threads)
+        om = oracle_workload_model(orc, n, L, st)
+        el = time_oracle_stages(om, 1, 3)
+        v = cells * 1.0 / el
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": (STAGE_SAMPLE % (n, threads, cpu_model())) + "; 3 samples (one RK3 step, %.1f s) "
+                         "after one warm-up stage" % el}
+        del om
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "maxwell_ion_256^3", "grid": [n, n, n], "box_L": L,
-                           "gamma": 50.0, "kappa": 2.0, "closure": "maxwell", "tau_model": "ichimaru",
-                           "transport": "yukawa_fit", "dt": dt, "precision": "fp32 fields, fp64 sums",
-                           "parallelism": "replicas" if world > 1 else "single",
-                           "l2": "inputs larger than L2 (working set ~GBs)", "tiles": tiles},
+                "config": workload_config(n, L, world),
+                "precision": "fp32 fields and transforms, fp64 conserved sums", "dt": dt, "tiles": tiles,
                 "roofline": roof,
                 "step_roofline": {"bytes_per_cell_step": STEP_BYTES_FP32,
                                   "achieved_GBps": STEP_BYTES_FP32 * value / world / 1e9,

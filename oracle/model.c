@@ -144,11 +144,20 @@ struct orc_model {
     double *dn, *dmom, *dpi, *dn_o, *dmom_o, *dpi_o;
     orc_cplx *nhat;
     double *tmpv;    /* 3 fields work for stress divergence */
+    double *gtmp;    /* 3 fields work for stress_pi0 */
+    orc_cplx *chat;  /* half-spectrum work of the RY convolution */
 };
 
 static long NC(const orc_model *m) { return (long)m->p.nx * m->p.ny * m->p.nz; }
 static long NH(const orc_model *m) { return (long)m->spc.g.nkx * m->p.ny * m->p.nz; }
 static double *dalloc(long n) { return (double *)calloc(n > 0 ? n : 1, sizeof(double)); }
+
+/* memcpy of n doubles split over the OpenMP threads */
+static void pcopy(double *dst, const double *src, long n)
+{
+#pragma omp parallel for schedule(static)
+    for (long q = 0; q < n; ++q) dst[q] = src[q];
+}
 
 /* fe_hartree.f90:56-64 */
 static double hartree_kernel(const term_t *t, double k)
@@ -252,11 +261,10 @@ int orc_model_term_add_mu(orc_model *m, int i, const double *n, const orc_cplx *
         for (long q = 0; q < nc; ++q) mu[q] = mu[q] + t->w[q];
         return 0;
     case ORC_TERM_RY: {     /* fe_correlation_ry.f90:64-80 */
-        orc_cplx *b = (orc_cplx *)malloc(sizeof(orc_cplx) * nh);
-        memcpy(b, nhat, sizeof(orc_cplx) * nh);
+        orc_cplx *b = m->chat;
+        pcopy((double *)b, (const double *)nhat, 2 * nh);
         b[0] = nhat[0] - t->n0;
         orc_spec_convolve(spc, t->ck, b, t->w);
-        free(b);
 #pragma omp parallel for schedule(static)
         for (long q = 0; q < nc; ++q) mu[q] = mu[q] - t->w[q] / t->beta;
         return 0;
@@ -375,18 +383,18 @@ static void stress_pi0(orc_model *m, const double *u, double *pi)
 {
     orc_spec *spc = &m->spc;
     const long nc = NC(m);
-    double *gtmp = dalloc(3 * nc);
+    double *gtmp = m->gtmp;
     for (int i = 1; i <= 3; ++i) {
         if (i <= spc->g.ndim) {
             orc_spec_grad(spc, u + (i - 1) * nc, gtmp);
             for (int j = 1; j <= 3; ++j)
-                memcpy(m->gu + nc * ((i - 1) + 3 * (j - 1)), gtmp + (j - 1) * nc, sizeof(double) * nc);
+                pcopy(m->gu + nc * ((i - 1) + 3 * (j - 1)), gtmp + (j - 1) * nc, nc);
         } else {
             for (int j = 1; j <= 3; ++j) memset(m->gu + nc * ((i - 1) + 3 * (j - 1)), 0, sizeof(double) * nc);
         }
     }
-    free(gtmp);
 #define GU(c, i, j) m->gu[(c) + nc * (((i) - 1) + 3 * ((j) - 1))]
+#pragma omp parallel for schedule(static)
     for (long c = 0; c < nc; ++c) {
         double divu = GU(c, 1, 1) + GU(c, 2, 2) + GU(c, 3, 3);
         for (int i = 1; i <= 3; ++i)
@@ -410,7 +418,7 @@ static void stress_divergence(orc_model *m, const double *pi, double *f)
             continue;
         }
         for (int j = 1; j <= 3; ++j)
-            memcpy(m->tmpv + (j - 1) * nc, pi + (idx[i - 1][j - 1] - 1) * nc, sizeof(double) * nc);
+            pcopy(m->tmpv + (j - 1) * nc, pi + (idx[i - 1][j - 1] - 1) * nc, nc);
         orc_spec_div(spc, m->tmpv, f + (i - 1) * nc);
     }
 }
@@ -618,6 +626,8 @@ orc_model *orc_model_create(const orc_params *pin, const orc_structure *st_in, i
     m->dn_o = dalloc(nc); m->dmom_o = dalloc(3 * nc); m->dpi_o = dalloc(6 * nc);
     m->nhat = (orc_cplx *)calloc(NH(m), sizeof(orc_cplx));
     m->tmpv = dalloc(3 * nc);
+    m->gtmp = dalloc(3 * nc);
+    m->chat = (orc_cplx *)calloc(NH(m), sizeof(orc_cplx));
     m->t = 0.0; m->step = 0;
     m->dt = p->dt;
     if (status) *status = 0;
@@ -641,7 +651,7 @@ void orc_model_destroy(orc_model *m)
     free(m->u); free(m->mu); free(m->gmu); free(m->flux); free(m->divf);
     free(m->wpi); free(m->pi0); free(m->pi0_old); free(m->fpi); free(m->gpi);
     free(m->dn); free(m->dmom); free(m->dpi); free(m->dn_o); free(m->dmom_o); free(m->dpi_o);
-    free(m->nhat); free(m->tmpv);
+    free(m->nhat); free(m->tmpv); free(m->gtmp); free(m->chat);
     free(m);
 }
 
@@ -674,7 +684,7 @@ int orc_model_rhs(orc_model *m, double t, double *dn, double *dmom, double *dpi)
     /* external force */
     if (m->ext_active && m->ext_time_dependent) vext_eval(m, t);
     /* dissipative stress */
-    if (m->evolve) memcpy(m->wpi, m->pi, sizeof(double) * 6 * nc);
+    if (m->evolve) pcopy(m->wpi, m->pi, 6 * nc);
     else stress_pi0(m, m->u, m->wpi);
     stress_divergence(m, m->wpi, m->fpi);
     /* momentum */
@@ -792,9 +802,9 @@ int orc_model_stage(orc_model *m, int s)
                 for (long q = 0; q < 6 * nc; ++q)
                     m->pi[q] = m->pi[q] + dt * (RK_A[s] * m->dpi[q] + RK_B[s] * m->dpi_o[q]);
         }
-        memcpy(m->dn_o, m->dn, sizeof(double) * nc);
-        memcpy(m->dmom_o, m->dmom, sizeof(double) * 3 * nc);
-        if (m->evolve) memcpy(m->dpi_o, m->dpi, sizeof(double) * 6 * nc);
+        pcopy(m->dn_o, m->dn, nc);
+        pcopy(m->dmom_o, m->dmom, 3 * nc);
+        if (m->evolve) pcopy(m->dpi_o, m->dpi, 6 * nc);
         double dts = (RK_A[s] + RK_B[s]) * dt;
         ts = ts + dts;
         if (m->evolve) {
