@@ -90,6 +90,20 @@ double orc_sm_viscosity(double gamma, double kappa)
     return 5.0 * SQRT3PI / (36.0 * pow(gamma, 2.5) * orc_sm_knm(4, g));
 }
 
+/* stanton_murillo.f90:105-108 (sm_g), 124-127: D* = sqrt(3 pi)/(12 Gamma^{5/2} K_11(g)) */
+double orc_sm_diffusion(double gamma, double kappa)
+{
+    double g = gamma * sqrt(kappa * kappa + 3.0 * gamma / (1.0 + 3.0 * gamma));
+    return SQRT3PI / (12.0 * pow(gamma, 2.5) * orc_sm_knm(1, g));
+}
+
+/* stanton_murillo.f90:136-139: K* = 25 sqrt(3 pi)/(48 Gamma^{5/2} K_22(g)) */
+double orc_sm_conductivity(double gamma, double kappa)
+{
+    double g = gamma * sqrt(kappa * kappa + 3.0 * gamma / (1.0 + 3.0 * gamma));
+    return 25.0 * SQRT3PI / (48.0 * pow(gamma, 2.5) * orc_sm_knm(4, g));
+}
+
 /* stanton_murillo.f90:143-154 */
 void orc_sm_electron_viscosity(double rs, double gamma, double theta, double lambda_tf,
                                double *eta_l, double *eta_cv, double *eta_sm)

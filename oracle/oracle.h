@@ -236,6 +236,8 @@ void orc_fit_driven_response(int n, const double *t, const orc_cplx *z, double w
 /* transport fits (stanton_murillo.f90) */
 double orc_sm_knm(int idx, double g);
 double orc_sm_viscosity(double gamma, double kappa);
+double orc_sm_diffusion(double gamma, double kappa);
+double orc_sm_conductivity(double gamma, double kappa);
 void orc_sm_electron_viscosity(double rs, double gamma, double theta, double lambda_tf,
                                double *eta_l, double *eta_cv, double *eta_sm);
 

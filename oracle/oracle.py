@@ -161,6 +161,11 @@ def lib():
         L.orc_sm_knm.argtypes = [_I, _D]
         L.orc_sm_viscosity.restype = _D
         L.orc_sm_viscosity.argtypes = [_D, _D]
+        L.orc_sm_diffusion.restype = _D
+        L.orc_sm_diffusion.argtypes = [_D, _D]
+        L.orc_sm_conductivity.restype = _D
+        L.orc_sm_conductivity.argtypes = [_D, _D]
+        L.orc_sm_electron_viscosity.argtypes = [_D, _D, _D, _D, _DP, _DP, _DP]
         L.orc_set_threads.argtypes = [_I]
         _lib = L
     return _lib
@@ -310,6 +315,66 @@ def structure_from_hnc(pot, n0, nr, rmax, tol, mix, maxiter, with_derivative=Fal
                     st.du_dgamma, bool(st.has_energy))
     lib().orc_structure_free(C.byref(st))
     return out
+
+
+def structure_from_file(path, kind, n0):
+    """structure_from_file (structure_source.f90:87-138): a two-column text
+    file (k, S(k)) for kind 's' or (k, c(k)) for kind 'c'; blank lines,
+    lines starting with '#' and lines whose first two entries are not
+    numbers are skipped; k must be positive and strictly increasing."""
+    kk, vv = [], []
+    with open(path) as f:
+        for line in f:
+            t = line.strip()
+            if not t or t.startswith("#"):
+                continue
+            parts = t.replace(",", " ").split()
+            try:
+                a = float(parts[0].replace("d", "e").replace("D", "e"))
+                b = float(parts[1].replace("d", "e").replace("D", "e"))
+            except (ValueError, IndexError):
+                continue
+            kk.append(a)
+            vv.append(b)
+    if len(kk) < 2:
+        raise ValueError("structure file has fewer than two data rows: " + path)
+    k = np.array(kk)
+    v = np.array(vv)
+    kind = kind[:1].lower()
+    if kind == "s":
+        c = (1.0 - 1.0 / v) / n0
+    elif kind == "c":
+        c = v
+    else:
+        raise ValueError("structure file kind must be s or c")
+    if np.any(k[1:] <= k[:-1]):
+        raise ValueError("structure file: k must be strictly increasing")
+    if k[0] <= 0.0:
+        raise ValueError("structure file: k must be positive")
+    return Structure(k, c, n0, 0.0, 0.0, False)
+
+
+# transport fits (stanton_murillo.f90)
+def sm_knm(idx, g):
+    return lib().orc_sm_knm(idx, g)
+
+
+def sm_viscosity(gamma, kappa):
+    return lib().orc_sm_viscosity(gamma, kappa)
+
+
+def sm_diffusion(gamma, kappa):
+    return lib().orc_sm_diffusion(gamma, kappa)
+
+
+def sm_conductivity(gamma, kappa):
+    return lib().orc_sm_conductivity(gamma, kappa)
+
+
+def sm_electron_viscosity(rs, gamma, theta, lambda_tf):
+    el, cv, sm = _D(), _D(), _D()
+    lib().orc_sm_electron_viscosity(rs, gamma, theta, lambda_tf, C.byref(el), C.byref(cv), C.byref(sm))
+    return el.value, cv.value, sm.value
 
 
 # ------------------------------------------------------------- params

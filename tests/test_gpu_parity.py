@@ -140,6 +140,15 @@ CASES = {
                                                vext="gaussian", vext_amplitude=0.05, vext_width=2.0),
     "electron_gaussian_2d": dict(ELEC, nx=32, ny=16, nz=1, lx=20.0, ly=10.0, closure="newtonian",
                                  vext="gaussian", vext_amplitude=0.02, vext_width=3.0),
+    # the transport fits (transport.f90:81-90): Stanton-Murillo ion viscosity
+    # and the electron viscosity interpolation
+    "ion_stanton_murillo_3d": dict(ION, nx=16, ny=8, nz=8, lx=20.0, ly=10.0, lz=10.0, gamma=2.0, kappa=0.5,
+                                   closure="newtonian", transport="stanton_murillo"),
+    "ion_stanton_murillo_maxwell": dict(ION, nx=16, ny=12, nz=8, lx=20.0, ly=15.0, lz=10.0, gamma=5.0,
+                                        kappa=1.0, closure="maxwell", tau_model="ichimaru",
+                                        transport="stanton_murillo"),
+    "electron_fit_3d": dict(ELEC, nx=16, ny=8, nz=8, lx=20.0, ly=10.0, lz=10.0, rs=1.86, theta=1.0,
+                            closure="newtonian", transport="electron_fit"),
 }
 
 
@@ -195,6 +204,42 @@ def test_advance_fp32(hg, orc, case):
     assert rel(g[1], o.mom) < TOL32, rel(g[1], o.mom)
     if m.has_pi:
         assert rel(g[2], o.pi) < TOL32, rel(g[2], o.pi)
+
+
+@pytest.mark.parametrize("kind", ["s", "c"])
+def test_structure_file_source_matches_oracle(hg, orc, tmp_path, kind):
+    """structure = 'file' (structure_source.f90:87-138) with an HNC table
+    written as S(k) or c(k): the GPU's c(k) table equals the oracle's read
+    of the same file, and rhs / 5-step advance match to 1e-10."""
+    n0 = 3.0 / (4.0 * np.pi)
+    st = orc.structure_from_hnc(orc.make_pot("yukawa", 10.0, 0.5), n0, 2048, 40.0, 1e-9, 0.2, 5000)
+    path = tmp_path / ("table_%s.dat" % kind)
+    col = 1.0 / (1.0 - n0 * st.c) if kind == "s" else st.c
+    with open(path, "w") as f:
+        f.write("# k  %s(k) from HNC\n" % ("S" if kind == "s" else "c"))
+        for k, v in zip(st.k, col):
+            f.write("%22.14e %22.14e\n" % (k, v))
+    kw = dict(kind="ion", gamma=10.0, kappa=0.5, nx=16, ny=8, nz=8, lx=20.0, ly=10.0, lz=10.0,
+              transport="yukawa_fit", closure="newtonian", dt=0.02)
+    m = hg.Model(hg.default_params(structure="file", structure_file=str(path), structure_kind=kind, **kw))
+    so = orc.structure_from_file(str(path), kind, n0)
+    k, c = m.structure()
+    assert k.size == so.k.size
+    assert np.abs(k - so.k).max() <= 1e-15 * so.k.max()
+    assert np.abs(c - so.c).max() <= 1e-14 * np.abs(so.c).max()
+    o = orc.Model(orc.params(**kw), so)
+    n, mom, pi = seeded_state(m)
+    m.set_state(n, mom, pi)
+    n2, mom2, pi2 = m.get_state()
+    o.set_state(n2, mom2, pi2)
+    dn, dmom, _ = m.rhs(0.1)
+    on, omom, _ = o.rhs(0.1)
+    assert rel(dn, on) < TOL64 and rel(dmom, omom) < TOL64
+    m.advance(5)
+    o.advance(5)
+    g = m.get_state()
+    assert rel(g[0], o.n) < TOL64 and rel(g[1], o.mom) < TOL64
+    m.close()
 
 
 def test_budgets_and_mode(hg, orc):
