@@ -180,14 +180,16 @@ def measured_peak():
 
 
 def profile_traffic(kernel, precision):
-    """dram bytes per launch of `kernel` from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "maxwell256_%s_kernels.md" % precision)
+    """DRAM read + write bytes of one launch of `kernel` from the committed
+    ncu summary of the step (profiles/maxwell256_<precision>_dram_per_kernel.md)."""
+    path = os.path.join(ROOT, "profiles", "maxwell256_%s_dram_per_kernel.md" % precision)
     try:
         with open(path) as f:
             for line in f:
                 if line.startswith("| %s |" % kernel):
                     cols = [c.strip() for c in line.strip().strip("|").split("|")]
-                    return float(cols[-1])
+                    if len(cols) == 2:
+                        return float(cols[1])
     except (OSError, ValueError, IndexError):
         pass
     return None
@@ -428,6 +430,100 @@ def run_batch_leg(torch, hg, count, steps, warmup, dev):
     return out
 
 
+def chi_members(hg, n, omegas, precision):
+    """The driven-response sweep: electrons r_s = 1, theta = 1 (Thomas-Fermi,
+    gradient, Hartree, RY), n^3 box of L = 40, constant eta = 0.2, driven
+    v_ext = 1e-4 cos(q.x - w t) at q = 2 pi/L (3, 0, 0), one member per w.
+    dt from compute_dt with cfl 0.8 (inside the RK3 limits the reference's
+    compute_dt builds in, model.f90:176-181), so that the 4000 steps span
+    t = 230, about seven damping times of the driven mode."""
+    return [dict(kind="electron", rs=1.0, theta=1.0, nx=n, ny=n, nz=n, lx=40.0, ly=40.0, lz=40.0,
+                 closure="newtonian", transport="constant", eta=0.2, vext="driven", vext_amplitude=1e-4,
+                 vext_mode=(3, 0, 0), vext_omega=float(w), hnc_nr=4096, hnc_rmax=80.0, cfl=0.8, dt=0.0,
+                 gpu_precision=precision) for w in omegas]
+
+
+def chi_linear(m, q, w):
+    """chi(q, w) = -q^2 n0 / (-w^2 + q^2 c^2(q) - i q^2 (eta_l/m) w/(1 - i w tau))
+    (linear_response.f90:59-76) from the model's own functional kernel K(q),
+    c^2 = n0 K(q)/m."""
+    n0, mass = m.scalar("n0"), m.scalar("mass")
+    eta_l = m.scalar("eta_l")
+    tau = m.scalar("tau") if m.has_pi else 0.0
+    c2 = n0 * m.kernel(q) / mass
+    den = -w * w + q * q * c2 - 1j * q * q * (eta_l / mass) * w / (1.0 - 1j * w * tau)
+    return -q * q * n0 / den
+
+
+def run_chi_leg(torch, hg, dev, n=128, nw=32, steps=4000, every=10):
+    """C3: the driven chi(k, w) sweep, nw drive frequencies in [0.5, 3] w_p
+    as one ensemble (one member per frequency), `steps` RK3 steps each, in
+    FP32 and in FP64.  chi from the steady response of the driven mode
+    (the window after 60 % of the run) against linear theory; FP32 against
+    FP64 per frequency and per field after the steps."""
+    omegas = np.linspace(0.5, 3.0, nw)
+    q = 2.0 * np.pi * 3 / 40.0
+    out = {"workload": "driven chi(k,w) sweep: %d electron runs (r_s 1, theta 1, TF + gradient + Hartree + RY), "
+                       "%d^3, L = 40, w in [0.5, 3] w_p, v_ext 1e-4 at q = 2 pi/L (3,0,0), %d RK3 steps each"
+                       % (nw, n, steps), "members": nw, "steps": steps}
+    states, chis = {}, {}
+    for prec in ("fp32", "fp64"):
+        b = hg.Batch([hg.default_params(**kw) for kw in chi_members(hg, n, omegas, prec)], device=dev)
+        try:
+            dt = None
+            for m in b.members:
+                m.set_state(np.full((n, n, n), m.scalar("n0")))
+                d = m.compute_dt()
+                dt = d if dt is None else min(dt, d)
+            for m in b.members:
+                m.set_time(0.0, dt)
+            stream = torch.cuda.ExternalStream(b.stream_ptr(), device=dev)
+            ts, zs = [], [[] for _ in omegas]
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            ms = 0.0
+            done = 0
+            while done < steps:
+                k = min(every, steps - done)
+                e0.record(stream)
+                b.advance(k)
+                e1.record(stream)
+                torch.cuda.synchronize(dev)
+                ms += e0.elapsed_time(e1)
+                done += k
+                ts.append(done * dt)
+                for i, m in enumerate(b.members):
+                    zs[i].append(m.mode(0, 3, 0, 0))
+            ts = np.array(ts)
+            sel = ts >= 0.6 * ts[-1]
+            errs, scat, chi = [], [], []
+            for i, w in enumerate(omegas):
+                z = np.array(zs[i])[sel] * np.exp(1j * w * ts[sel])
+                a = z.mean()
+                chi_sim = 2.0 * a / 1e-4
+                chi_lin = chi_linear(b.members[i], q, w)
+                chi.append(chi_sim)
+                errs.append(abs(chi_sim - chi_lin) / abs(chi_lin))
+                scat.append(float(np.abs(z - a).max() / abs(a)))
+            chis[prec] = np.array(chi)
+            states[prec] = [m.get_state() for m in b.members]
+            out[prec] = {"value": nw * float(n) ** 3 * steps / (ms * 1e-3), "unit": UNIT,
+                         "ms_per_ensemble_step": ms / steps, "dt": dt, "t_end": steps * dt,
+                         "chi_rel_err_vs_linear_max": float(max(errs)), "chi_rel_err_vs_linear": [float(e) for e in errs],
+                         "transient_scatter_max": float(max(scat)), "grouped": b.grouped()}
+        finally:
+            b.close()
+    fe = []
+    for s32, s64 in zip(states["fp32"], states["fp64"]):
+        n0 = s64[0].mean()
+        fe.append(max(float(np.linalg.norm(s32[0] - s64[0]) / np.linalg.norm(s64[0])),
+                      float(np.linalg.norm(s32[1] - s64[1]) / np.linalg.norm(s64[1]))))
+    out["fp32_rel_err_vs_fp64_max"] = max(fe)
+    out["chi_fp32_vs_fp64_max"] = float(np.max(np.abs(chis["fp32"] - chis["fp64"]) / np.abs(chis["fp64"])))
+    out["omegas"] = [float(w) for w in omegas]
+    return out
+
+
 # even 2^a 3^b lengths in [32, 256] (the GPU path's FFT lengths)
 SERVE_SIZES = [32, 36, 48, 54, 64, 72, 96, 108, 128, 144, 162, 192, 216, 256]
 
@@ -532,9 +628,11 @@ def main():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--batch-members", type=int, default=256,
                     help="also time the ensemble workload with this many members (0: skip)")
-    ap.add_argument("--workload", default="maxwell256", choices=["maxwell256", "batch", "serve"],
+    ap.add_argument("--workload", default="maxwell256", choices=["maxwell256", "batch", "serve", "chi"],
                     help="batch: time only the ensemble workload (256 members unless --batch-members); "
                          "serve: the serving stream at --rates")
+    ap.add_argument("--chi-omegas", type=int, default=32, help="chi sweep: drive frequencies")
+    ap.add_argument("--chi-steps", type=int, default=4000, help="chi sweep: RK3 steps per run")
     ap.add_argument("--rates", default="10,30,100,300,1000", help="serving arrival rates (requests/s)")
     ap.add_argument("--per-rate", type=int, default=6, help="serving requests per rate")
     ap.add_argument("--step-scale", type=float, default=1.0, help="serving steps scale (1: 500-5000)")
@@ -550,6 +648,12 @@ def main():
         torch.cuda.set_device(dev)
         res = run_serve_leg(hg, dev, [float(x) for x in args.rates.split(",")], args.per_rate, args.step_scale)
         print(json.dumps(res), flush=True)
+        return 0
+    if args.workload == "chi":
+        dev = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(dev)
+        print(json.dumps(run_chi_leg(torch, hg, dev, n=args.n if args.n != 256 else 128,
+                                     nw=args.chi_omegas, steps=args.chi_steps)), flush=True)
         return 0
     if args.workload == "batch":
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
@@ -641,8 +745,8 @@ def main():
             "frac": achieved / peak, "peak_source": peak_kind, "share": dms / tot,
             "bytes_per_launch": dbytes, "avg_launch_ms": dms / dn,
             "traffic": profile_traffic(dname, "fp32"),
-            "traffic_source": "profiles/maxwell256_fp32_kernels.md (ncu dram bytes of one full-size launch, "
-                              "committed capture; not measured in this run)"}
+            "traffic_source": "profiles/maxwell256_fp32_dram_per_kernel.md (ncu dram read + write bytes of one "
+                              "full-size launch, committed capture; not measured in this run)"}
     kernels = {k: {"ms_per_step": v[0] / 2, "launches_per_step": v[2] / 2,
                    "GBps": (v[1] / (v[0] / v[2] * 1e-3) / 1e9) if v[0] > 0 and v[1] > 0 else None}
                for k, v in prof.items()}

@@ -27,6 +27,17 @@
 
 using namespace hydft;
 
+// Members whose steps record the same launches (kernel kinds and shapes)
+// step together: each launch of the step runs once for the whole group, on
+// the group's stream, with the members' arguments in a device table.
+struct EnsembleGroup {
+    std::vector<int> members;
+    std::vector<LaunchRec> recs;     // the first member's launches (kinds and shapes)
+    std::vector<size_t> tab_off;     // offset of each launch's pack table in the table buffer
+    cudaStream_t st = nullptr;
+    cudaEvent_t done = nullptr;
+};
+
 struct hydft_batch {
     std::vector<hydft_gpu *> m;
     int device = 0;
@@ -35,7 +46,12 @@ struct hydft_batch {
     std::vector<cudaEvent_t> join;
     cudaGraphExec_t gexec = nullptr;
     std::vector<int64_t> gens;           // member graph generations at capture
-    std::vector<int64_t> step_launches;  // kernels of one member step
+    std::vector<int64_t> step_launches;  // kernels of one member step, as the member alone would launch them
+    std::vector<EnsembleGroup> groups;
+    std::vector<int> solo;               // members stepping on their own stream (no ensemble form)
+    void *dtab = nullptr;                // the groups' pack tables (device)
+    int64_t graph_kernels = 0;           // kernels per graph launch
+    int64_t launches = 0;                // kernels launched by this ensemble's graph so far
     unsigned *hstat = nullptr;           // pinned status words, one per member
     int failed = -1;
     std::string err;
@@ -75,25 +91,134 @@ void destroy_member(hydft_gpu *h)
     delete h;
 }
 
+void drop_groups(hydft_batch *b)
+{
+    for (auto &g : b->groups) {
+        if (g.done) cudaEventDestroy(g.done);
+        if (g.st) cudaStreamDestroy(g.st);
+    }
+    b->groups.clear();
+    b->solo.clear();
+    if (b->dtab) cudaFree(b->dtab);
+    b->dtab = nullptr;
+}
+
 void drop_graph(hydft_batch *b)
 {
     if (b->gexec) cudaGraphExecDestroy(b->gexec);
     b->gexec = nullptr;
 }
 
-// one graph: fork -> every member's step on its stream -> join
+// the launch kinds and shapes of a recorded step, as a grouping key
+std::string step_signature(const std::vector<LaunchRec> &recs)
+{
+    std::string k;
+    char buf[160];
+    for (const LaunchRec &r : recs) {
+        std::snprintf(buf, sizeof buf, "%p:%u,%u,%u:%u,%u,%u:%zu:%zu;", r.kind, r.grid.x, r.grid.y, r.grid.z, r.block.x,
+                      r.block.y, r.block.z, r.smem, r.pack.size());
+        k += buf;
+    }
+    return k;
+}
+
+// Records every member's step, groups members with the same launches and
+// builds their pack tables; members without an ensemble form step alone.
+int build_groups(hydft_batch *b)
+{
+    drop_groups(b);
+    const size_t n = b->m.size();
+    std::vector<std::vector<LaunchRec>> recs(n);
+    std::map<std::string, size_t> key_to_group;
+    for (size_t i = 0; i < n; ++i) {
+        const int rc = b->m[i]->s->record_step(recs[i]);
+        if (rc == HYDFT_ERR_UNSUPPORTED) {
+            b->solo.push_back((int)i);
+            continue;
+        }
+        if (rc) return fail(b, rc, "member " + std::to_string(i) + ": " + b->m[i]->s->err);
+        const std::string key = step_signature(recs[i]);
+        auto it = key_to_group.find(key);
+        if (it == key_to_group.end()) {
+            key_to_group[key] = b->groups.size();
+            b->groups.emplace_back();
+            b->groups.back().recs = recs[i];
+            it = key_to_group.find(key);
+        }
+        b->groups[it->second].members.push_back((int)i);
+    }
+    // one table per launch per group: the members' packs back to back
+    size_t total = 0;
+    for (auto &g : b->groups) {
+        g.tab_off.resize(g.recs.size());
+        for (size_t r = 0; r < g.recs.size(); ++r) {
+            g.tab_off[r] = total;
+            total += (g.recs[r].pack.size() * g.members.size() + 255) / 256 * 256;
+        }
+    }
+    if (total) {
+        std::vector<unsigned char> host(total, 0);
+        for (auto &g : b->groups)
+            for (size_t r = 0; r < g.recs.size(); ++r) {
+                const size_t sz = g.recs[r].pack.size();
+                for (size_t j = 0; j < g.members.size(); ++j)
+                    std::memcpy(host.data() + g.tab_off[r] + j * sz, recs[g.members[j]][r].pack.data(), sz);
+            }
+        if (cudaMalloc(&b->dtab, total) != cudaSuccess) return fail(b, HYDFT_ERR_OOM, "ensemble: pack tables");
+        cudaError_t e = cudaMemcpy(b->dtab, host.data(), total, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return fail(b, HYDFT_ERR_CUDA, std::string("ensemble: pack tables: ") + cudaGetErrorString(e));
+    }
+    for (auto &g : b->groups) {
+        if (cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming) != cudaSuccess)
+            return fail(b, HYDFT_ERR_CUDA, "ensemble: group stream or event creation failed");
+        for (const LaunchRec &r : g.recs) {
+            cudaError_t e = r.prepare(r.smem);
+            if (e != cudaSuccess) return fail(b, HYDFT_ERR_CUDA, std::string("ensemble: ") + cudaGetErrorString(e));
+        }
+        for (int i : g.members) b->step_launches[i] = (int64_t)recs[i].size();
+    }
+    return HYDFT_OK;
+}
+
+// one graph: fork -> each group's launches on its stream, and each member
+// without an ensemble form on its own stream -> join
 int capture(hydft_batch *b)
 {
     drop_graph(b);
     const size_t n = b->m.size();
     for (size_t i = 0; i < n; ++i)
         if (int rc = b->m[i]->s->prepare()) return fail(b, rc, "member " + std::to_string(i) + ": " + b->m[i]->s->err);
+    if (int rc = build_groups(b)) return rc;
     std::vector<int64_t> before(n);
     for (size_t i = 0; i < n; ++i) before[i] = b->m[i]->s->launches;
     cudaError_t e = cudaStreamBeginCapture(b->root, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return fail(b, HYDFT_ERR_CUDA, std::string("begin capture: ") + cudaGetErrorString(e));
     cudaEventRecord(b->fork, b->root);
-    for (size_t i = 0; i < n; ++i) {
+    int64_t kernels = 0;
+    for (auto &g : b->groups) {
+        cudaStreamWaitEvent(g.st, b->fork, 0);
+        for (size_t r = 0; r < g.recs.size(); ++r) {
+            const LaunchRec &lr = g.recs[r];
+            lr.launch(static_cast<unsigned char *>(b->dtab) + g.tab_off[r], (unsigned)g.members.size(), lr.grid, lr.block,
+                      lr.smem, g.st);
+            const cudaError_t le = cudaGetLastError();
+            if (le != cudaSuccess) {
+                cudaGraph_t dead = nullptr;
+                cudaStreamEndCapture(b->root, &dead);
+                if (dead) cudaGraphDestroy(dead);
+                char buf[256];
+                std::snprintf(buf, sizeof buf, "ensemble launch %zu (%s) of %zu members, grid %u x %u x %u, block %u, "
+                              "%zu bytes shared: ", r, lr.name, g.members.size(), lr.grid.x, lr.grid.y, lr.grid.z,
+                              lr.block.x, lr.smem);
+                return fail(b, HYDFT_ERR_CUDA, buf + std::string(cudaGetErrorString(le)));
+            }
+        }
+        kernels += (int64_t)g.recs.size();
+        cudaEventRecord(g.done, g.st);
+        cudaStreamWaitEvent(b->root, g.done, 0);
+    }
+    for (int i : b->solo) {
         cudaStream_t s = static_cast<cudaStream_t>(b->m[i]->s->stream());
         cudaStreamWaitEvent(s, b->fork, 0);
         b->m[i]->s->enqueue_steps(1);
@@ -106,11 +231,13 @@ int capture(hydft_batch *b)
     e = cudaGraphInstantiate(&b->gexec, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return fail(b, HYDFT_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
-    for (size_t i = 0; i < n; ++i) {
+    for (int i : b->solo) {
         b->step_launches[i] = b->m[i]->s->launches - before[i];
         b->m[i]->s->launches = before[i];
-        b->gens[i] = b->m[i]->s->graph_gen;
+        kernels += b->step_launches[i];
     }
+    for (size_t i = 0; i < n; ++i) b->gens[i] = b->m[i]->s->graph_gen;
+    b->graph_kernels = kernels;
     return HYDFT_OK;
 }
 
@@ -258,6 +385,7 @@ void hydft_batch_destroy(hydft_batch *b)
     cudaSetDevice(b->device);
     if (b->root) cudaStreamSynchronize(b->root);
     drop_graph(b);
+    drop_groups(b);
     for (auto *h : b->m) destroy_member(h);
     for (auto e : b->join)
         if (e) cudaEventDestroy(e);
@@ -311,6 +439,7 @@ int hydft_batch_advance(hydft_batch *b, int nsteps)
         cudaError_t e = cudaGraphLaunch(b->gexec, b->root);
         if (e != cudaSuccess) return fail(b, HYDFT_ERR_CUDA, std::string("graph launch: ") + cudaGetErrorString(e));
     }
+    b->launches += b->graph_kernels * nsteps;
     for (size_t i = 0; i < n; ++i) {
         b->m[i]->s->launches += b->step_launches[i] * nsteps;
         cudaMemcpyAsync(b->hstat + i, b->m[i]->s->status_word(), sizeof(unsigned), cudaMemcpyDeviceToHost, b->root);
@@ -335,12 +464,16 @@ int hydft_batch_advance(hydft_batch *b, int nsteps)
     return HYDFT_OK;
 }
 
-int64_t hydft_batch_launch_count(const hydft_batch *b)
+int64_t hydft_batch_launch_count(const hydft_batch *b) { return b ? b->launches : 0; }
+
+int hydft_batch_grouped(const hydft_batch *b, int *groups, int *members)
 {
-    if (!b) return 0;
-    int64_t t = 0;
-    for (auto *h : b->m) t += h->s->launches;
-    return t;
+    if (!b) return HYDFT_ERR_BAD_ARG;
+    int nm = 0;
+    for (const auto &g : b->groups) nm += (int)g.members.size();
+    if (groups) *groups = (int)b->groups.size();
+    if (members) *members = nm;
+    return HYDFT_OK;
 }
 
 void *hydft_batch_stream(const hydft_batch *b) { return b ? (void *)b->root : nullptr; }

@@ -72,4 +72,40 @@ struct Grid {
 __host__ __device__ __forceinline__ int signed_idx(int c, int M) { return c <= M ? c : c - (2 * M + 1); }
 __host__ __device__ __forceinline__ int fft_idx(int m, int n) { return m >= 0 ? m : m + n; }
 
+// Block coordinates and grid extent of one simulation's share of a launch.
+// A plain launch uses the hardware's.  An ensemble launch runs one kernel
+// for many simulations of the same shape: their grids are stacked along z,
+// and each block finds its simulation and its coordinates in that
+// simulation's grid (ensemble_kernel below).
+struct BlockIx {
+    unsigned x, y, z;
+    unsigned gx, gy, gz;
+};
+
+__device__ __forceinline__ BlockIx hw_block()
+{
+    return BlockIx{blockIdx.x, blockIdx.y, blockIdx.z, gridDim.x, gridDim.y, gridDim.z};
+}
+
+// The ensemble form of a kernel.  P (a "pack") holds one simulation's
+// launch arguments and runs the kernel body for one block of that
+// simulation's grid; tab[m] is simulation m's pack (in device memory) and
+// zper the z extent of one simulation's grid, so block z = m zper + z'.
+// Each block first copies its simulation's pack into shared memory: the
+// body then reads its arguments from an address space that its global
+// stores cannot alias, so they are loaded once rather than after every
+// store.  A model on its own runs the same kernel with one pack.
+template <class P>
+__global__ void __launch_bounds__(P::MAXT, P::MINB) ensemble_kernel(const P *__restrict__ tab, unsigned zper)
+{
+    static_assert(sizeof(P) % 8 == 0 && alignof(P) <= 8, "packs are copied in 8-byte words");
+    __shared__ __align__(16) unsigned long long sp[sizeof(P) / 8];
+    const unsigned m = blockIdx.z / zper;
+    const unsigned long long *src = reinterpret_cast<const unsigned long long *>(tab + m);
+    for (unsigned i = threadIdx.x; i < sizeof(P) / 8; i += blockDim.x) sp[i] = src[i];
+    __syncthreads();
+    const BlockIx b{blockIdx.x, blockIdx.y, blockIdx.z - m * zper, gridDim.x, gridDim.y, zper};
+    reinterpret_cast<const P *>(sp)->run(b);
+}
+
 }  // namespace hydft

@@ -498,7 +498,8 @@ __host__ __device__ __forceinline__ int pi_idx(int i, int j)
 // NM: the number of momentum components (1, 2, 3) as a compile-time
 // constant, so that every small per-mode array below stays in registers
 template <typename R, int NM>
-__global__ void combine_a_kernel(Grid g, Phys ph, CombineA<R> c, Ctrl *ctrl, int stage)
+__device__ __forceinline__ void combine_a_body(const BlockIx &bk, const Grid &g, const Phys &ph, const CombineA<R> &c,
+                                               Ctrl *ctrl, int stage)
 {
     constexpr int nm = NM;
     const size_t total = (size_t)g.nkzc * g.nkyc * g.pkx;
@@ -508,8 +509,8 @@ __global__ void combine_a_kernel(Grid g, Phys ph, CombineA<R> c, Ctrl *ctrl, int
     const int nf = nm * (nm + 1) / 2;
     const bool need_u = ph.evolve || ph.newtonian;
     const cplx<R> zero = {R(0), R(0)};
-    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
-         idx += (size_t)gridDim.x * blockDim.x) {
+    for (size_t idx = bk.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (size_t)bk.gx * blockDim.x) {
         int kxc, kyc, kzc;
         kvec(g, idx, kxc, kyc, kzc);
         if (kxc >= g.nkxc) continue;
@@ -613,6 +614,24 @@ __global__ void combine_a_kernel(Grid g, Phys ph, CombineA<R> c, Ctrl *ctrl, int
     }
 }
 
+template <typename R, int NM>
+__global__ void combine_a_kernel(const __grid_constant__ Grid g, const __grid_constant__ Phys ph,
+                                 const __grid_constant__ CombineA<R> c, Ctrl *ctrl, int stage)
+{
+    combine_a_body<R, NM>(hw_block(), g, ph, c, ctrl, stage);
+}
+
+template <typename R, int NM>
+struct CombineAPack {
+    static constexpr int MAXT = 256, MINB = 2;
+    Grid g;
+    Phys ph;
+    CombineA<R> c;
+    Ctrl *ctrl;
+    int stage;
+    __device__ __forceinline__ void run(const BlockIx &b) const { combine_a_body<R, NM>(b, g, ph, c, ctrl, stage); }
+};
+
 template <typename R>
 struct CombineB {
     cplx<R> *N, *M[3], *P[6];        // state (updated in place)
@@ -622,7 +641,8 @@ struct CombineB {
 };
 
 template <typename R, int NM>
-__global__ void combine_b_kernel(Grid g, Phys ph, CombineB<R> c, Ctrl *ctrl, int stage, int rhs_only)
+__device__ __forceinline__ void combine_b_body(const BlockIx &bk, const Grid &g, const Phys &ph, const CombineB<R> &c,
+                                               Ctrl *ctrl, int stage, int rhs_only)
 {
     constexpr int nm = NM;
     const size_t total = (size_t)g.nkzc * g.nkyc * g.pkx;
@@ -631,8 +651,8 @@ __global__ void combine_b_kernel(Grid g, Phys ph, CombineB<R> c, Ctrl *ctrl, int
     const R da = R(dt * s.a), db = R(dt * s.b);
     const cplx<R> zero = {R(0), R(0)};
     const bool regs = !rhs_only && stage != 0;   // the RK registers are read
-    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
-         idx += (size_t)gridDim.x * blockDim.x) {
+    for (size_t idx = bk.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (size_t)bk.gx * blockDim.x) {
         int kxc, kyc, kzc;
         kvec(g, idx, kxc, kyc, kzc);
         if (kxc >= g.nkxc) continue;
@@ -714,12 +734,33 @@ __global__ void combine_b_kernel(Grid g, Phys ph, CombineB<R> c, Ctrl *ctrl, int
             }
         }
     }
-    if (!rhs_only && blockIdx.x == 0 && threadIdx.x == 0 && ph.evolve) {
+    if (!rhs_only && bk.x == 0 && threadIdx.x == 0 && ph.evolve) {
         ctrl->pending = 1;
         ctrl->pend_phi = s.phi;
         ctrl->pend_e = s.e;
     }
 }
+
+template <typename R, int NM>
+__global__ void combine_b_kernel(const __grid_constant__ Grid g, const __grid_constant__ Phys ph,
+                                 const __grid_constant__ CombineB<R> c, Ctrl *ctrl, int stage, int rhs_only)
+{
+    combine_b_body<R, NM>(hw_block(), g, ph, c, ctrl, stage, rhs_only);
+}
+
+template <typename R, int NM>
+struct CombineBPack {
+    static constexpr int MAXT = 256, MINB = 2;
+    Grid g;
+    Phys ph;
+    CombineB<R> c;
+    Ctrl *ctrl;
+    int stage, rhs_only;
+    __device__ __forceinline__ void run(const BlockIx &b) const
+    {
+        combine_b_body<R, NM>(b, g, ph, c, ctrl, stage, rhs_only);
+    }
+};
 
 // Completes a pending relaxation from u of the current state (combine U).
 template <typename R>
@@ -764,10 +805,10 @@ __global__ void combine_u_kernel(Grid g, Phys ph, CombineU<R> c, Ctrl *ctrl)
 }
 
 // Per-step scalars: stage times, drive amplitude and phase, relaxation factors.
-static __global__ void begin_step_kernel(Ctrl *ctrl, double tau, int ext_td, double amp0, double omega,
-                                  double ramp)
+__device__ __forceinline__ void begin_step_body(const BlockIx &bk, Ctrl *ctrl, double tau, int ext_td, double amp0,
+                                                double omega, double ramp)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (threadIdx.x != 0 || bk.x != 0) return;
     const double A[3] = {32.0 / 60.0, 25.0 / 60.0, 45.0 / 60.0};
     const double Bc[3] = {0.0, -17.0 / 60.0, -25.0 / 60.0};
     double ts = ctrl->t;
@@ -797,9 +838,27 @@ static __global__ void begin_step_kernel(Ctrl *ctrl, double tau, int ext_td, dou
     }
 }
 
-static __global__ void end_step_kernel(Ctrl *ctrl)
+static __global__ void begin_step_kernel(Ctrl *ctrl, double tau, int ext_td, double amp0, double omega,
+                                         double ramp)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    begin_step_body(hw_block(), ctrl, tau, ext_td, amp0, omega, ramp);
+}
+
+struct BeginStepPack {
+    static constexpr int MAXT = 32, MINB = 1;
+    Ctrl *ctrl;
+    double tau;
+    int ext_td;
+    double amp0, omega, ramp;
+    __device__ __forceinline__ void run(const BlockIx &b) const
+    {
+        begin_step_body(b, ctrl, tau, ext_td, amp0, omega, ramp);
+    }
+};
+
+__device__ __forceinline__ void end_step_body(const BlockIx &bk, Ctrl *ctrl)
+{
+    if (threadIdx.x != 0 || bk.x != 0) return;
     ctrl->t = ctrl->t + ctrl->dt;
     ctrl->step = ctrl->step + 1;
     // the last right-hand side of the step was evaluated at stage 3's time
@@ -807,6 +866,14 @@ static __global__ void end_step_kernel(Ctrl *ctrl)
     ctrl->v_ewr = ctrl->st[2].ewr;
     ctrl->v_ewi = ctrl->st[2].ewi;
 }
+
+static __global__ void end_step_kernel(Ctrl *ctrl) { end_step_body(hw_block(), ctrl); }
+
+struct EndStepPack {
+    static constexpr int MAXT = 32, MINB = 1;
+    Ctrl *ctrl;
+    __device__ __forceinline__ void run(const BlockIx &b) const { end_step_body(b, ctrl); }
+};
 
 // one probe record: t, n and mom_x at compact index idx (conjugated when
 // the mode is stored as its mirror), into ring slot *count

@@ -127,14 +127,14 @@ __device__ __forceinline__ void store_block(cplx<R> *__restrict__ col, const cpl
 // z passes: NB ky rows (G apart) per thread, all NB columns loaded before the
 // first is transformed, so that a thread keeps NB x E loads in flight
 template <typename R, int T, int E, int TX, int G, bool BAND, int NB>
-__global__ void __launch_bounds__(TX * T * G) zinv_fast(Grid g, PassArgs<R> a, const cplx<R> *twz)
+__device__ __forceinline__ void zinv_body(const BlockIx &bk, const Grid &g, const PassArgs<R> &a, const cplx<R> *twz)
 {
     constexpr int L = T * E;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
     cplx<R> *xb = tw + 2 * L;
     const int tid = threadIdx.x, c = tid % TX, t = (tid / TX) % T, gi = tid / (TX * T);
-    const int x = blockIdx.x * TX + c, f = blockIdx.z;
+    const int x = bk.x * TX + c, f = bk.z;
     const int op = a.op[f];
     for (int i = tid; i < 2 * L; i += blockDim.x) tw[i] = twz[i];
     const R kx = R(x * g.kx0);
@@ -144,13 +144,13 @@ __global__ void __launch_bounds__(TX * T * G) zinv_fast(Grid g, PassArgs<R> a, c
     cplx<R> v[NB][E];
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
-        const int kyc = (blockIdx.y * NB + b) * G + gi;
+        const int kyc = (bk.y * NB + b) * G + gi;
         const bool valid = x < g.nkxc && kyc < g.nkyc;
         load_band<R, T, E, BAND>(v[b], a.in[f] + (size_t)kyc * g.pkx + x, rs, t, g.Mz, g.nkzc, valid);
     }
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
-        const int kyc = (blockIdx.y * NB + b) * G + gi;
+        const int kyc = (bk.y * NB + b) * G + gi;
         const bool valid = x < g.nkxc && kyc < g.nkyc;
         const int my = valid ? signed_idx(kyc, g.My) : 0;
         const R ky = R(my * g.ky0);
@@ -191,15 +191,30 @@ __global__ void __launch_bounds__(TX * T * G) zinv_fast(Grid g, PassArgs<R> a, c
     }
 }
 
+template <typename R, int T, int E, int TX, int G, bool BAND, int NB>
+__global__ void __launch_bounds__(TX * T * G) zinv_fast(const __grid_constant__ Grid g, const __grid_constant__ PassArgs<R> a, const cplx<R> *twz)
+{
+    zinv_body<R, T, E, TX, G, BAND, NB>(hw_block(), g, a, twz);
+}
+
+template <typename R, int T, int E, int TX, int G, bool BAND, int NB>
+struct ZinvPack {
+    static constexpr int MAXT = TX * T * G, MINB = 1;
+    Grid g;
+    PassArgs<R> a;
+    const cplx<R> *tw;
+    __device__ __forceinline__ void run(const BlockIx &b) const { zinv_body<R, T, E, TX, G, BAND, NB>(b, g, a, tw); }
+};
+
 template <typename R, int T, int E, int TX, int G, bool BAND>
-__global__ void __launch_bounds__(TX * T * G) yinv_fast(Grid g, PassArgs<R> a, const cplx<R> *twy)
+__device__ __forceinline__ void yinv_body(const BlockIx &bk, const Grid &g, const PassArgs<R> &a, const cplx<R> *twy)
 {
     constexpr int L = T * E;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
     cplx<R> *xb = tw + 2 * L;
     const int tid = threadIdx.x, c = tid % TX, t = (tid / TX) % T, gi = tid / (TX * T);
-    const int x = blockIdx.x * TX + c, z = blockIdx.y * G + gi, f = blockIdx.z;
+    const int x = bk.x * TX + c, z = bk.y * G + gi, f = bk.z;
     const bool valid = x < g.nkxc && z < g.nz;
     for (int i = tid; i < 2 * L; i += blockDim.x) tw[i] = twy[i];
     cplx<R> v[E];
@@ -218,14 +233,29 @@ __global__ void __launch_bounds__(TX * T * G) yinv_fast(Grid g, PassArgs<R> a, c
 }
 
 template <typename R, int T, int E, int TX, int G, bool BAND>
-__global__ void __launch_bounds__(TX * T * G) yfwd_fast(Grid g, PassArgs<R> a, const cplx<R> *twy)
+__global__ void __launch_bounds__(TX * T * G) yinv_fast(const __grid_constant__ Grid g, const __grid_constant__ PassArgs<R> a, const cplx<R> *twy)
+{
+    yinv_body<R, T, E, TX, G, BAND>(hw_block(), g, a, twy);
+}
+
+template <typename R, int T, int E, int TX, int G, bool BAND>
+struct YinvPack {
+    static constexpr int MAXT = TX * T * G, MINB = 1;
+    Grid g;
+    PassArgs<R> a;
+    const cplx<R> *tw;
+    __device__ __forceinline__ void run(const BlockIx &b) const { yinv_body<R, T, E, TX, G, BAND>(b, g, a, tw); }
+};
+
+template <typename R, int T, int E, int TX, int G, bool BAND>
+__device__ __forceinline__ void yfwd_body(const BlockIx &bk, const Grid &g, const PassArgs<R> &a, const cplx<R> *twy)
 {
     constexpr int L = T * E;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
     cplx<R> *xb = tw + 2 * L;
     const int tid = threadIdx.x, c = tid % TX, t = (tid / TX) % T, gi = tid / (TX * T);
-    const int x = blockIdx.x * TX + c, z = blockIdx.y * G + gi, f = blockIdx.z;
+    const int x = bk.x * TX + c, z = bk.y * G + gi, f = bk.z;
     const bool valid = x < g.nkxc && z < g.nz;
     for (int i = tid; i < 2 * L; i += blockDim.x) tw[i] = twy[i];
     cplx<R> v[E];
@@ -235,33 +265,64 @@ __global__ void __launch_bounds__(TX * T * G) yfwd_fast(Grid g, PassArgs<R> a, c
     if (valid) store_band<R, T, E, BAND>(a.out[f] + (size_t)z * g.nkyc * g.pkx + x, v, g.pkx, t, g.My, g.nkyc, R(1));
 }
 
+template <typename R, int T, int E, int TX, int G, bool BAND>
+__global__ void __launch_bounds__(TX * T * G) yfwd_fast(const __grid_constant__ Grid g, const __grid_constant__ PassArgs<R> a, const cplx<R> *twy)
+{
+    yfwd_body<R, T, E, TX, G, BAND>(hw_block(), g, a, twy);
+}
+
+template <typename R, int T, int E, int TX, int G, bool BAND>
+struct YfwdPack {
+    static constexpr int MAXT = TX * T * G, MINB = 1;
+    Grid g;
+    PassArgs<R> a;
+    const cplx<R> *tw;
+    __device__ __forceinline__ void run(const BlockIx &b) const { yfwd_body<R, T, E, TX, G, BAND>(b, g, a, tw); }
+};
+
 template <typename R, int T, int E, int TX, int G, bool BAND, int NB>
-__global__ void __launch_bounds__(TX * T * G) zfwd_fast(Grid g, PassArgs<R> a, const cplx<R> *twz, R norm)
+__device__ __forceinline__ void zfwd_body(const BlockIx &bk, const Grid &g, const PassArgs<R> &a, const cplx<R> *twz, R norm)
 {
     constexpr int L = T * E;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<R> *tw = reinterpret_cast<cplx<R> *>(smraw);
     cplx<R> *xb = tw + 2 * L;
     const int tid = threadIdx.x, c = tid % TX, t = (tid / TX) % T, gi = tid / (TX * T);
-    const int x = blockIdx.x * TX + c, f = blockIdx.z;
+    const int x = bk.x * TX + c, f = bk.z;
     for (int i = tid; i < 2 * L; i += blockDim.x) tw[i] = twz[i];
     const int rs = g.nkyc * g.pkx;
     cplx<R> v[NB][E];
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
-        const int kyc = (blockIdx.y * NB + b) * G + gi;
+        const int kyc = (bk.y * NB + b) * G + gi;
         const bool valid = x < g.nkxc && kyc < g.nkyc;
         load_block<R, T, E>(v[b], a.in[f] + (size_t)kyc * g.pkx + x, rs, t, valid);
     }
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
-        const int kyc = (blockIdx.y * NB + b) * G + gi;
+        const int kyc = (bk.y * NB + b) * G + gi;
         const bool valid = x < g.nkxc && kyc < g.nkyc;
         if (b == 0) __syncthreads();   // the twiddles (later rows: the exchange's own barriers)
         block_to_stride<T, E, -1, R, BarBlock, TX>(v[b], t, xb + gi * (L + L / T) * TX + c, tw);
         if (valid) store_band<R, T, E, BAND>(a.out[f] + (size_t)kyc * g.pkx + x, v[b], rs, t, g.Mz, g.nkzc, norm);
     }
 }
+
+template <typename R, int T, int E, int TX, int G, bool BAND, int NB>
+__global__ void __launch_bounds__(TX * T * G) zfwd_fast(const __grid_constant__ Grid g, const __grid_constant__ PassArgs<R> a, const cplx<R> *twz, R norm)
+{
+    zfwd_body<R, T, E, TX, G, BAND, NB>(hw_block(), g, a, twz, norm);
+}
+
+template <typename R, int T, int E, int TX, int G, bool BAND, int NB>
+struct ZfwdPack {
+    static constexpr int MAXT = TX * T * G, MINB = 1;
+    Grid g;
+    PassArgs<R> a;
+    const cplx<R> *tw;
+    R norm;
+    __device__ __forceinline__ void run(const BlockIx &b) const { zfwd_body<R, T, E, TX, G, BAND, NB>(b, g, a, tw, norm); }
+};
 
 // smem bytes of a y/z fast pass
 template <typename R>
@@ -405,7 +466,8 @@ __host__ __device__ constexpr int flux_j3(int f) { return f < 3 ? f : (f < 5 ? f
 #endif
 
 template <typename R, int T, int E, int NM, bool GRAD, bool UONLY>
-__global__ void __launch_bounds__(256, HYDFT_XMINB) xa_fast(Grid g, XFastArgs<R> a, const cplx<R> *twx, PWA<R> pw)
+__device__ __forceinline__ void xa_fast_body(const BlockIx &bk, const Grid &g, const XFastArgs<R> &a,
+    const cplx<R> *twx, const PWA<R> &pw)
 {
     static_assert(NM == 3, "fast x pass is for 3-D grids");
     constexpr int L = T * E;
@@ -421,7 +483,7 @@ __global__ void __launch_bounds__(256, HYDFT_XMINB) xa_fast(Grid g, XFastArgs<R>
     R *muslot = reinterpret_cast<R *>(slots + NP * E * nt);
     R *invslot = muslot + E * nt;
     const int tid = threadIdx.x, t = tid % T, rr = tid / T;
-    const int row = blockIdx.x * rb + rr;
+    const int row = bk.x * rb + rr;
     const bool rowok = row < g.ny * g.nz;
     cplx<R> *xrow = xbuf + rr * xrow_stride<T, E>();
     for (int i = tid; i < 2 * L; i += nt) tw[i] = twx[i];
@@ -516,11 +578,29 @@ __global__ void __launch_bounds__(256, HYDFT_XMINB) xa_fast(Grid g, XFastArgs<R>
     }
 }
 
+template <typename R, int T, int E, int NM, bool GRAD, bool UONLY>
+__global__ void __launch_bounds__(256, HYDFT_XMINB) xa_fast(const __grid_constant__ Grid g, const __grid_constant__ XFastArgs<R> a,
+    const cplx<R> *twx, const __grid_constant__ PWA<R> pw)
+{
+    xa_fast_body<R, T, E, NM, GRAD, UONLY>(hw_block(), g, a, twx, pw);
+}
+
+template <typename R, int T, int E, int NM, bool GRAD, bool UONLY>
+struct XaFastPack {
+    static constexpr int MAXT = 256, MINB = HYDFT_XMINB;
+    Grid g;
+    XFastArgs<R> a;
+    const cplx<R> *tw;
+    PWA<R> pw;
+    __device__ __forceinline__ void run(const BlockIx &b) const { xa_fast_body<R, T, E, NM, GRAD, UONLY>(b, g, a, tw, pw); }
+};
+
 // Phase B: inputs [d mu/dx_0 ..], then for each Pi component pair (c, c+1)
 // and d < NM the pair (d Pi_c/dx_d, d Pi_{c+1}/dx_d); outputs
 // n (d mu/dx_i - F_i) and, when Pi evolves, -u.grad Pi_c.
 template <typename R, int T, int E, int NM, bool EVOLVE>
-__global__ void __launch_bounds__(256, HYDFT_XMINB) xb_fast(Grid g, XFastArgs<R> a, const cplx<R> *twx, PWB<R> pw)
+__device__ __forceinline__ void xb_fast_body(const BlockIx &bk, const Grid &g, const XFastArgs<R> &a,
+    const cplx<R> *twx, const PWB<R> &pw)
 {
     constexpr int L = T * E;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -528,7 +608,7 @@ __global__ void __launch_bounds__(256, HYDFT_XMINB) xb_fast(Grid g, XFastArgs<R>
     cplx<R> *xbuf = tw + 2 * L;
     const int nt = blockDim.x, rb = nt / T;
     const int tid = threadIdx.x, t = tid % T, rr = tid / T;
-    const int row = blockIdx.x * rb + rr;
+    const int row = bk.x * rb + rr;
     const bool rowok = row < g.ny * g.nz;
     cplx<R> *xrow = xbuf + rr * xrow_stride<T, E>();
     for (int i = tid; i < 2 * L; i += nt) tw[i] = twx[i];
@@ -587,6 +667,23 @@ __global__ void __launch_bounds__(256, HYDFT_XMINB) xb_fast(Grid g, XFastArgs<R>
         }
     }
 }
+
+template <typename R, int T, int E, int NM, bool EVOLVE>
+__global__ void __launch_bounds__(256, HYDFT_XMINB) xb_fast(const __grid_constant__ Grid g, const __grid_constant__ XFastArgs<R> a,
+    const cplx<R> *twx, const __grid_constant__ PWB<R> pw)
+{
+    xb_fast_body<R, T, E, NM, EVOLVE>(hw_block(), g, a, twx, pw);
+}
+
+template <typename R, int T, int E, int NM, bool EVOLVE>
+struct XbFastPack {
+    static constexpr int MAXT = 256, MINB = HYDFT_XMINB;
+    Grid g;
+    XFastArgs<R> a;
+    const cplx<R> *tw;
+    PWB<R> pw;
+    __device__ __forceinline__ void run(const BlockIx &b) const { xb_fast_body<R, T, E, NM, EVOLVE>(b, g, a, tw, pw); }
+};
 
 // 16-byte asynchronous global -> shared copies (cp.async, sm_80 and later);
 // the wait only covers this thread's own committed copies, so it ends.
@@ -654,7 +751,8 @@ __host__ __device__ constexpr int xstaged_minb() { return sizeof(R) == 4 && E <=
 // first: (mu_local, u_0), (u_1, u_2), (m0u0, m0u1), (m0u2, m1u1), (m1u2, m2u2);
 // UONLY: (u_0, u_1), (u_2, -).  Outputs go to the same fields as xa_fast's.
 template <typename R, int T, int E, bool UONLY, bool BAND>
-__global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xa_regs(Grid g, XFastArgs<R> a, const cplx<R> *twx, PWA<R> pw)
+__device__ __forceinline__ void xa_regs_body(const BlockIx &bk, const Grid &g, const XFastArgs<R> &a,
+    const cplx<R> *twx, const PWA<R> &pw)
 {
     constexpr int L = T * E;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -663,7 +761,7 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xa_regs(Grid g, XFa
     cplx<R> *sb = tw + 2 * L;                      // [4][rb][pkx] the staged inputs
     cplx<R> *xbuf = sb + 4 * (size_t)rb * pk;
     const int tid = threadIdx.x, t = tid % T, rr = tid / T;
-    const int row0 = blockIdx.x * rb, row = row0 + rr;
+    const int row0 = bk.x * rb, row = row0 + rr;
     const bool rowok = row < g.ny * g.nz;
     const int vrows = max(0, min(rb, g.ny * g.nz - row0));
     cplx<R> *xrow = xbuf + rr * xrow_stride<T, E>();
@@ -754,6 +852,23 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xa_regs(Grid g, XFa
     }
 }
 
+template <typename R, int T, int E, bool UONLY, bool BAND>
+__global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xa_regs(const __grid_constant__ Grid g, const __grid_constant__ XFastArgs<R> a,
+    const cplx<R> *twx, const __grid_constant__ PWA<R> pw)
+{
+    xa_regs_body<R, T, E, UONLY, BAND>(hw_block(), g, a, twx, pw);
+}
+
+template <typename R, int T, int E, bool UONLY, bool BAND>
+struct XaRegsPack {
+    static constexpr int MAXT = 256, MINB = xstaged_minb<R, E>();
+    Grid g;
+    XFastArgs<R> a;
+    const cplx<R> *tw;
+    PWA<R> pw;
+    __device__ __forceinline__ void run(const BlockIx &b) const { xa_regs_body<R, T, E, UONLY, BAND>(b, g, a, tw, pw); }
+};
+
 // row stride (elements) of the staged real rows: one row of x plus T, so
 // that the rows read by one warp start in different bank groups
 template <int T, int E>
@@ -768,7 +883,8 @@ __host__ __device__ constexpr int xreal_stride() { return T * E + T; }
 // and are differentiated here on the way in.  EXTK: no external force (0), a
 // plane-wave potential (1), the gaussian potential's static force field (2).
 template <typename R, int T, int E, bool EVOLVE, int EXTK, bool BAND>
-__global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xb_rows(Grid g, XFastArgs<R> a, const cplx<R> *twx, PWB<R> pw)
+__device__ __forceinline__ void xb_rows_body(const BlockIx &bk, const Grid &g, const XFastArgs<R> &a,
+    const cplx<R> *twx, const PWB<R> &pw)
 {
     constexpr int L = T * E, NM = 3;
     constexpr int RS = xreal_stride<T, E>();
@@ -784,7 +900,7 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xb_rows(Grid g, XFa
     R *rs = reinterpret_cast<R *>(xbuf + rb * xrow_stride<T, E>());   // [3][rb][RS] u rows
     const int tid = threadIdx.x, t = tid % T, rr = tid / T;
     const int nrows = g.ny * g.nz;
-    const int row0 = blockIdx.x * rb;
+    const int row0 = bk.x * rb;
     const int row = row0 + rr;
     const bool rowok = row < nrows;
     cplx<R> *xrow = xbuf + rr * xrow_stride<T, E>();
@@ -892,6 +1008,23 @@ __global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xb_rows(Grid g, XFa
         }
     }
 }
+
+template <typename R, int T, int E, bool EVOLVE, int EXTK, bool BAND>
+__global__ void __launch_bounds__(256, xstaged_minb<R, E>()) xb_rows(const __grid_constant__ Grid g, const __grid_constant__ XFastArgs<R> a,
+    const cplx<R> *twx, const __grid_constant__ PWB<R> pw)
+{
+    xb_rows_body<R, T, E, EVOLVE, EXTK, BAND>(hw_block(), g, a, twx, pw);
+}
+
+template <typename R, int T, int E, bool EVOLVE, int EXTK, bool BAND>
+struct XbRowsPack {
+    static constexpr int MAXT = 256, MINB = xstaged_minb<R, E>();
+    Grid g;
+    XFastArgs<R> a;
+    const cplx<R> *tw;
+    PWB<R> pw;
+    __device__ __forceinline__ void run(const BlockIx &b) const { xb_rows_body<R, T, E, EVOLVE, EXTK, BAND>(b, g, a, tw, pw); }
+};
 
 // shared-memory bytes of the staged x passes: twiddles, staged spectral
 // rows (nstage fields), exchange rows, staged real rows (nreal fields)

@@ -47,6 +47,25 @@ struct KernelStat {
     int64_t n = 0;        // launches
 };
 
+// One kernel launch of a step in the form an ensemble replays it: the
+// kernel (kind identifies its pack type), its launch shape for one
+// simulation, and the launch arguments (the pack) as bytes.  An ensemble
+// groups simulations whose steps record the same kinds and shapes, copies
+// their packs into one device table per launch and runs each launch once
+// for the whole group (ensemble_kernel in common.cuh).
+struct LaunchRec {
+    const void *kind = nullptr;
+    const char *name = nullptr;
+    double bytes = 0.0;
+    dim3 grid, block;
+    size_t smem = 0;
+    std::vector<unsigned char> pack;
+    // the ensemble form for n simulations whose packs are at tab (device)
+    void (*launch)(const void *tab, unsigned n, dim3 grid, dim3 block, size_t smem, cudaStream_t st) = nullptr;
+    // raises the ensemble form's dynamic shared-memory limit to smem
+    cudaError_t (*prepare)(size_t smem) = nullptr;
+};
+
 class SolverBase {
 public:
     virtual ~SolverBase() {}
@@ -84,6 +103,10 @@ public:
     virtual void tiles(int *t5) const = 0;
     // axes whose passes classify band elements at compile time (x 1, y 2, z 4)
     virtual int band_axes() const = 0;
+    // Records the launches of one RK3 step (after tuning) without running
+    // them.  Returns HYDFT_ERR_UNSUPPORTED, with out empty, when a launch of
+    // the step has no ensemble form (that simulation then steps on its own).
+    virtual int record_step(std::vector<LaunchRec> &out) = 0;
     // records that steps enqueued earlier (a replayed ensemble graph) ran
     virtual void mark_advanced() = 0;
     // k replays of the captured step graph on this solver's stream, without

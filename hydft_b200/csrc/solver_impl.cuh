@@ -43,7 +43,7 @@ namespace hydft {
     } while (0)
 
 enum { HYDFT_E_OK = 0, HYDFT_E_BAD = 1, HYDFT_E_OOM = 2, HYDFT_E_NONPOS = 3, HYDFT_E_NONFINITE = 4,
-       HYDFT_E_NEWTON = 5, HYDFT_E_CUDA = 7 };
+       HYDFT_E_NEWTON = 5, HYDFT_E_CUDA = 7, HYDFT_E_UNSUPPORTED = 8 };
 
 // reduction partials of the diagnostics kernel
 struct RedPart {
@@ -378,6 +378,22 @@ static bool has_plan(int L)
     return L == 32 || L == 48 || L == 64 || L == 96 || L == 128 || L == 256;
 }
 
+// The ensemble form of pack P's kernel for n simulations (LaunchRec::launch)
+template <class P>
+void ensemble_launch(const void *tab, unsigned n, dim3 grid, dim3 block, size_t smem, cudaStream_t st)
+{
+    static_assert(std::is_trivially_copyable<P>::value, "a pack is copied as bytes");
+    ensemble_kernel<P><<<dim3(grid.x, grid.y, grid.z * n), block, smem, st>>>(static_cast<const P *>(tab), grid.z);
+}
+
+// the dynamic shared-memory limit of the ensemble form; its static copy of
+// the pack counts against the default 48 KB, so the limit is always set
+template <class P>
+cudaError_t ensemble_prepare(size_t smem)
+{
+    return cudaFuncSetAttribute(ensemble_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
 template <typename R>
 class Solver : public SolverBase {
 public:
@@ -454,9 +470,20 @@ public:
     std::vector<EvRec> evrecs;
     bool profiling = false;
 
+    // set while record_step runs: launches are recorded, not run
+    std::vector<LaunchRec> *rec = nullptr;
+    bool rec_ok = true;
+    // this solver's step packs (the ensemble-of-one form of its step)
+    void *packbuf = nullptr;
+    size_t packcap = 0;
+
     template <class F>
     void launch(const char *name, double bytes, F &&f)
     {
+        if (rec) {   // a launch without an ensemble form
+            rec_ok = false;
+            return;
+        }
         cudaEvent_t a = nullptr, b = nullptr;
         if (profiling) {
             cudaEventCreate(&a);
@@ -481,6 +508,29 @@ public:
         }
     }
 
+    // a launch with an ensemble form: pack P holds its arguments, f runs the
+    // plain kernel
+    template <class P, class F>
+    void launch_p(const char *name, double bytes, dim3 grid, dim3 block, size_t smem, const P &pack, F &&f)
+    {
+        if (rec) {
+            LaunchRec r;
+            r.kind = reinterpret_cast<const void *>(&ensemble_launch<P>);
+            r.name = name;
+            r.bytes = bytes;
+            r.grid = grid;
+            r.block = block;
+            r.smem = smem;
+            r.pack.resize(sizeof(P));
+            std::memcpy(r.pack.data(), &pack, sizeof(P));
+            r.launch = &ensemble_launch<P>;
+            r.prepare = &ensemble_prepare<P>;
+            rec->push_back(std::move(r));
+            return;
+        }
+        launch(name, bytes, f);
+    }
+
     double cb() const { return 2.0 * sizeof(R); }   // bytes of one complex value
 
     int precision_bits() const override { return sizeof(R) * 8; }
@@ -500,6 +550,7 @@ public:
         if (gexec) cudaGraphExecDestroy(gexec);
         if (graph) cudaGraphDestroy(graph);
         for (void *p : allocs) cudaFree(p);
+        if (packbuf) cudaFree(packbuf);
         if (st) cudaStreamDestroy(st);
     }
 
@@ -813,11 +864,19 @@ public:
             constexpr int TX = decltype(TXc)::value;
             constexpr int G = yz_rows<T, TX, decltype(NTc)::value>();
             const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
-            auto k = z_nb == 2 ? (band_z ? zinv_fast<R, T, E, TX, G, true, 2> : zinv_fast<R, T, E, TX, G, false, 2>)
-                               : (band_z ? zinv_fast<R, T, E, TX, G, true, 1> : zinv_fast<R, T, E, TX, G, false, 1>);
-            set_smem(k, sm);
-            const dim3 grid((g.nkxc + TX - 1) / TX, (g.nkyc + G * z_nb - 1) / (G * z_nb), nzf);
-            launch("zinv", zbytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, a, tpz); });
+            auto go = [&](auto k, auto pk, int nb) {
+                set_smem(k, sm);
+                const dim3 grid((g.nkxc + TX - 1) / TX, (g.nkyc + G * nb - 1) / (G * nb), nzf);
+                pk.g = g; pk.a = a; pk.tw = tpz;
+                launch_p("zinv", zbytes, grid, TX * T * G, sm, pk, [&] { k<<<grid, TX * T * G, sm, st>>>(g, a, tpz); });
+            };
+            if (z_nb == 2) {
+                if (band_z) go(zinv_fast<R, T, E, TX, G, true, 2>, ZinvPack<R, T, E, TX, G, true, 2>{}, 2);
+                else go(zinv_fast<R, T, E, TX, G, false, 2>, ZinvPack<R, T, E, TX, G, false, 2>{}, 2);
+            } else {
+                if (band_z) go(zinv_fast<R, T, E, TX, G, true, 1>, ZinvPack<R, T, E, TX, G, true, 1>{}, 1);
+                else go(zinv_fast<R, T, E, TX, G, false, 1>, ZinvPack<R, T, E, TX, G, false, 1>{}, 1);
+            }
             });
         });
         if (!zf) {
@@ -841,10 +900,14 @@ public:
                 constexpr int TX = decltype(TXc)::value;
                 constexpr int G = yz_rows<T, TX, decltype(NTc)::value>();
                 const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
-                auto k = band_y ? yinv_fast<R, T, E, TX, G, true> : yinv_fast<R, T, E, TX, G, false>;
-                set_smem(k, sm);
                 const dim3 grid((g.nkxc + TX - 1) / TX, (g.nz + G - 1) / G, nf);
-                launch("yinv", ybytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, b, tpy); });
+                auto go = [&](auto k, auto pk) {
+                    set_smem(k, sm);
+                    pk.g = g; pk.a = b; pk.tw = tpy;
+                    launch_p("yinv", ybytes, grid, TX * T * G, sm, pk, [&] { k<<<grid, TX * T * G, sm, st>>>(g, b, tpy); });
+                };
+                if (band_y) go(yinv_fast<R, T, E, TX, G, true>, YinvPack<R, T, E, TX, G, true>{});
+                else go(yinv_fast<R, T, E, TX, G, false>, YinvPack<R, T, E, TX, G, false>{});
             });
             });
             if (!yf) {
@@ -875,10 +938,14 @@ public:
                 constexpr int TX = decltype(TXc)::value;
                 constexpr int G = yz_rows<T, TX, decltype(NTc)::value>();
                 const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
-                auto k = band_y ? yfwd_fast<R, T, E, TX, G, true> : yfwd_fast<R, T, E, TX, G, false>;
-                set_smem(k, sm);
                 const dim3 grid((g.nkxc + TX - 1) / TX, (g.nz + G - 1) / G, nf);
-                launch("yfwd", ybytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, b, tpy); });
+                auto go = [&](auto k, auto pk) {
+                    set_smem(k, sm);
+                    pk.g = g; pk.a = b; pk.tw = tpy;
+                    launch_p("yfwd", ybytes, grid, TX * T * G, sm, pk, [&] { k<<<grid, TX * T * G, sm, st>>>(g, b, tpy); });
+                };
+                if (band_y) go(yfwd_fast<R, T, E, TX, G, true>, YfwdPack<R, T, E, TX, G, true>{});
+                else go(yfwd_fast<R, T, E, TX, G, false>, YfwdPack<R, T, E, TX, G, false>{});
             });
             });
             if (!yf) {
@@ -902,11 +969,19 @@ public:
             constexpr int TX = decltype(TXc)::value;
             constexpr int G = yz_rows<T, TX, decltype(NTc)::value>();
             const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
-            auto k = z_nbf == 2 ? (band_z ? zfwd_fast<R, T, E, TX, G, true, 2> : zfwd_fast<R, T, E, TX, G, false, 2>)
-                                : (band_z ? zfwd_fast<R, T, E, TX, G, true, 1> : zfwd_fast<R, T, E, TX, G, false, 1>);
-            set_smem(k, sm);
-            const dim3 grid((g.nkxc + TX - 1) / TX, (g.nkyc + G * z_nbf - 1) / (G * z_nbf), nf);
-            launch("zfwd", zbytes, [&] { k<<<grid, TX * T * G, sm, st>>>(g, a, tpz, norm); });
+            auto go = [&](auto k, auto pk, int nb) {
+                set_smem(k, sm);
+                const dim3 grid((g.nkxc + TX - 1) / TX, (g.nkyc + G * nb - 1) / (G * nb), nf);
+                pk.g = g; pk.a = a; pk.tw = tpz; pk.norm = norm;
+                launch_p("zfwd", zbytes, grid, TX * T * G, sm, pk, [&] { k<<<grid, TX * T * G, sm, st>>>(g, a, tpz, norm); });
+            };
+            if (z_nbf == 2) {
+                if (band_z) go(zfwd_fast<R, T, E, TX, G, true, 2>, ZfwdPack<R, T, E, TX, G, true, 2>{}, 2);
+                else go(zfwd_fast<R, T, E, TX, G, false, 2>, ZfwdPack<R, T, E, TX, G, false, 2>{}, 2);
+            } else {
+                if (band_z) go(zfwd_fast<R, T, E, TX, G, true, 1>, ZfwdPack<R, T, E, TX, G, true, 1>{}, 1);
+                else go(zfwd_fast<R, T, E, TX, G, false, 1>, ZfwdPack<R, T, E, TX, G, false, 1>{}, 1);
+            }
             });
         });
         if (!zf) {
@@ -953,38 +1028,45 @@ public:
         const int nrows = g.ny * g.nz;
         with_plan(g.nx, [&](auto Tc, auto Ec) {
             constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value;
-            auto go = [&](auto k, int np) {
+            auto go = [&](auto k, auto pk, int np) {
                 size_t sm;
                 const int nt = x_threads<T, E>(np, sm);
                 set_smem(k, sm);
                 const int rb = nt / T;
-                launch(name, xbytes(nin, nout, nreal), [&] { k<<<(nrows + rb - 1) / rb, nt, sm, st>>>(g, a, tpx, pw); });
+                const dim3 grid((nrows + rb - 1) / rb);
+                pk.g = g; pk.a = a; pk.tw = tpx; pk.pw = pw;
+                launch_p(name, xbytes(nin, nout, nreal), grid, nt, sm, pk, [&] { k<<<grid, nt, sm, st>>>(g, a, tpx, pw); });
             };
-            auto go_regs = [&](auto k) {
+            auto go_regs = [&](auto k, auto pk) {
                 int nt = std::min(256, x_ntmax) / T * T;
                 size_t sm = xstaged_smem<R, T, E>(nt, g.pkx, 4, 0);
                 // the blocks per SM the kernel is compiled for must fit: 228 KB
-                // of shared memory per SM, 1 KB reserved per block
-                const size_t cap = xstaged_minb<R, E>() == 2 ? 115712 : (size_t)smem_optin;
+                // of shared memory per SM, 1 KB reserved per block, and the
+                // ensemble form's copy of its pack
+                const size_t cap = (xstaged_minb<R, E>() == 2 ? 115712 : (size_t)smem_optin) - sizeof(pk);
                 while (sm > cap && nt > T) {
                     nt /= 2;
                     sm = xstaged_smem<R, T, E>(nt, g.pkx, 4, 0);
                 }
                 set_smem(k, sm);
                 const int rb = nt / T;
-                launch(name, xbytes(nin, nout, nreal), [&] { k<<<(nrows + rb - 1) / rb, nt, sm, st>>>(g, a, tpx, pw); });
+                const dim3 grid((nrows + rb - 1) / rb);
+                pk.g = g; pk.a = a; pk.tw = tpx; pk.pw = pw;
+                launch_p(name, xbytes(nin, nout, nreal), grid, nt, sm, pk, [&] { k<<<grid, nt, sm, st>>>(g, a, tpx, pw); });
             };
             const bool no_fd = !ph.has_tf && !ph.has_grad;
             if (staged_x && uonly) {
-                go_regs(band_x ? xa_regs<R, T, E, true, true> : xa_regs<R, T, E, true, false>);
+                if (band_x) go_regs(xa_regs<R, T, E, true, true>, XaRegsPack<R, T, E, true, true>{});
+                else go_regs(xa_regs<R, T, E, true, false>, XaRegsPack<R, T, E, true, false>{});
             } else if (staged_x && !grad && no_fd) {
-                go_regs(band_x ? xa_regs<R, T, E, false, true> : xa_regs<R, T, E, false, false>);
+                if (band_x) go_regs(xa_regs<R, T, E, false, true>, XaRegsPack<R, T, E, false, true>{});
+                else go_regs(xa_regs<R, T, E, false, false>, XaRegsPack<R, T, E, false, false>{});
             } else if (uonly) {
-                go(xa_fast<R, T, E, 3, false, true>, 2);
+                go(xa_fast<R, T, E, 3, false, true>, XaFastPack<R, T, E, 3, false, true>{}, 2);
             } else if (grad) {
-                go(xa_fast<R, T, E, 3, true, false>, 4);
+                go(xa_fast<R, T, E, 3, true, false>, XaFastPack<R, T, E, 3, true, false>{}, 4);
             } else {
-                go(xa_fast<R, T, E, 3, false, false>, 2);
+                go(xa_fast<R, T, E, 3, false, false>, XaFastPack<R, T, E, 3, false, false>{}, 2);
             }
         });
     }
@@ -996,30 +1078,36 @@ public:
         const int nrows = g.ny * g.nz;
         with_plan(g.nx, [&](auto Tc, auto Ec) {
             constexpr int T = decltype(Tc)::value, E = decltype(Ec)::value;
-            auto go = [&](auto k) {
+            auto go = [&](auto k, auto pk) {
                 size_t sm;
                 const int nt = x_threads<T, E>(0, sm);
                 set_smem(k, sm);
                 const int rb = nt / T;
-                launch("xpass_b", xbytes(nin, nout, nreal), [&] { k<<<(nrows + rb - 1) / rb, nt, sm, st>>>(g, a, tpx, pw); });
+                const dim3 grid((nrows + rb - 1) / rb);
+                pk.g = g; pk.a = a; pk.tw = tpx; pk.pw = pw;
+                launch_p("xpass_b", xbytes(nin, nout, nreal), grid, nt, sm, pk, [&] { k<<<grid, nt, sm, st>>>(g, a, tpx, pw); });
             };
-            auto go_rows = [&](auto k, int nreal_rows) {
+            auto go_rows = [&](auto k, auto pk, int nreal_rows) {
                 int nt = std::min(256, x_ntmax) / T * T;
                 size_t sm = xstaged_smem<R, T, E>(nt, g.pkx, 2, nreal_rows);
-                // two blocks per SM: 228 KB of shared memory, 1 KB reserved per block
-                while (sm > 115712 && nt > T) {
+                // two blocks per SM: 228 KB of shared memory, 1 KB reserved per
+                // block, and the ensemble form's copy of its pack
+                while (sm > 115712 - sizeof(pk) && nt > T) {
                     nt /= 2;
                     sm = xstaged_smem<R, T, E>(nt, g.pkx, 2, nreal_rows);
                 }
                 set_smem(k, sm);
                 const int rb = nt / T;
-                launch("xpass_b", xbytes(nin, nout, nreal), [&] { k<<<(nrows + rb - 1) / rb, nt, sm, st>>>(g, a, tpx, pw); });
+                const dim3 grid((nrows + rb - 1) / rb);
+                pk.g = g; pk.a = a; pk.tw = tpx; pk.pw = pw;
+                launch_p("xpass_b", xbytes(nin, nout, nreal), grid, nt, sm, pk, [&] { k<<<grid, nt, sm, st>>>(g, a, tpx, pw); });
             };
             const int extk = !ph.ext_active ? 0 : (ph.ext_kind == 3 ? 2 : 1);
             auto rows = [&](auto ev, auto ek) {
                 constexpr bool EV = decltype(ev)::value;
                 constexpr int EK = decltype(ek)::value;
-                go_rows(band_x ? xb_rows<R, T, E, EV, EK, true> : xb_rows<R, T, E, EV, EK, false>, EV ? 3 : 0);
+                if (band_x) go_rows(xb_rows<R, T, E, EV, EK, true>, XbRowsPack<R, T, E, EV, EK, true>{}, EV ? 3 : 0);
+                else go_rows(xb_rows<R, T, E, EV, EK, false>, XbRowsPack<R, T, E, EV, EK, false>{}, EV ? 3 : 0);
             };
             using std::integral_constant;
             using EvT = integral_constant<bool, true>;
@@ -1033,9 +1121,9 @@ public:
                 else if (extk == 1) rows(EvF{}, integral_constant<int, 1>{});
                 else rows(EvF{}, integral_constant<int, 0>{});
             } else if (ph.evolve) {
-                go(xb_fast<R, T, E, 3, true>);
+                go(xb_fast<R, T, E, 3, true>, XbFastPack<R, T, E, 3, true>{});
             } else {
-                go(xb_fast<R, T, E, 3, false>);
+                go(xb_fast<R, T, E, 3, false>, XbFastPack<R, T, E, 3, false>{});
             }
         });
     }
@@ -1126,8 +1214,13 @@ public:
         for (int d = 0; d < 3; ++d) c.Q[d] = Q[d];
         const double ncomp = (double)g.nkxc * g.nkyc * g.nkzc;
         const int nrw = 2 + nm + nm * (nm + 1) / 2 + 1 + nm + (ph.evolve ? 24 : 0);
-        launch("combine_a", ncomp * (cb() * nrw + sizeof(R)),
-               [&] { with_nm([&](auto n) { combine_a_kernel<R, decltype(n)::value><<<combine_grid(), 256, 0, st>>>(g, ph, c, ctrl, stage); }); });
+        with_nm([&](auto n) {
+            constexpr int NMc = decltype(n)::value;
+            const dim3 grid(combine_grid());
+            const CombineAPack<R, NMc> pk{g, ph, c, ctrl, stage};
+            launch_p("combine_a", ncomp * (cb() * nrw + sizeof(R)), grid, 256, 0, pk,
+                     [&] { combine_a_kernel<R, NMc><<<grid, 256, 0, st>>>(g, ph, c, ctrl, stage); });
+        });
     }
 
     // phase B's inverse transforms into YI buffers 0..nf-1; returns nf.
@@ -1218,19 +1311,22 @@ public:
         }
         const double ncomp = (double)g.nkxc * g.nkyc * g.nkzc;
         const int nrw = 2 + 5 * nm + 2 + (ph.evolve ? 30 : 0);
-        launch("combine_b", ncomp * cb() * nrw, [&] {
-            with_nm([&](auto n) {
-                combine_b_kernel<R, decltype(n)::value><<<combine_grid(), 256, 0, st>>>(g, ph, c, ctrl, stage, rhs_only ? 1 : 0);
-            });
+        with_nm([&](auto n) {
+            constexpr int NMc = decltype(n)::value;
+            const dim3 grid(combine_grid());
+            const int ro = rhs_only ? 1 : 0;
+            const CombineBPack<R, NMc> pk{g, ph, c, ctrl, stage, ro};
+            launch_p("combine_b", ncomp * cb() * nrw, grid, 256, 0, pk,
+                     [&] { combine_b_kernel<R, NMc><<<grid, 256, 0, st>>>(g, ph, c, ctrl, stage, ro); });
         });
     }
 
     void begin_step()
     {
         const double omega = S.ext_kind == 2 ? S.ext_omega : 0.0;
-        launch("step_ctrl", 0.0, [&] {
-            begin_step_kernel<<<1, 32, 0, st>>>(ctrl, ph.evolve ? ph.tau : 0.0, S.ext_td, S.ext_amp, omega,
-                                                S.ext_ramp);
+        const BeginStepPack pk{ctrl, ph.evolve ? ph.tau : 0.0, S.ext_td, S.ext_amp, omega, S.ext_ramp};
+        launch_p("step_ctrl", 0.0, dim3(1), 32, 0, pk, [&] {
+            begin_step_kernel<<<1, 32, 0, st>>>(pk.ctrl, pk.tau, pk.ext_td, pk.amp0, pk.omega, pk.ramp);
         });
     }
 
@@ -1241,7 +1337,8 @@ public:
             phase_a(s, ph.evolve != 0);
             phase_b(s, false);
         }
-        launch("step_ctrl", 0.0, [&] { end_step_kernel<<<1, 32, 0, st>>>(ctrl); });
+        const EndStepPack pk{ctrl};
+        launch_p("step_ctrl", 0.0, dim3(1), 32, 0, pk, [&] { end_step_kernel<<<1, 32, 0, st>>>(ctrl); });
     }
 
     // Maxwell: complete the last stage's relaxation from u of the new state
@@ -1314,7 +1411,16 @@ public:
         kstats.clear();
         evrecs.clear();
         profiling = true;
-        for (int i = 0; i < nsteps; ++i) one_step();
+        for (int i = 0; i < nsteps; ++i) {
+            std::vector<LaunchRec> recs;
+            std::vector<size_t> off;
+            int rc = 0;
+            CK(cudaStreamSynchronize(st));   // the pack table is rewritten for every step
+            const bool ens = upload_recorded(recs, off, rc);
+            if (rc) { profiling = false; return rc; }
+            if (ens) launch_recorded(recs, off);
+            else one_step();
+        }
         host_pending = ph.evolve != 0;
         profiling = false;
         CK(cudaStreamSynchronize(st));
@@ -1366,6 +1472,37 @@ public:
     }
 
     int band_axes() const override { return (band_x ? 1 : 0) | (band_y ? 2 : 0) | (band_z ? 4 : 0); }
+
+    // Grids of at least this many cells step with the plain kernels (their
+    // arguments in the constant bank) alone and in ensembles: their launches
+    // fill the GPU by themselves, and the ensemble form, which reads its
+    // arguments from memory, holds them in registers (up to 25 % more per
+    // thread in the transform passes).  Smaller grids step with the
+    // ensemble form alone too, so that a model alone and the same model in
+    // an ensemble group run the same kernels (bit-identical fields).
+    // HYDFT_ENSEMBLE_MAX_CELLS overrides the 128^3 default.
+    static size_t ensemble_max_cells()
+    {
+        const char *e = std::getenv("HYDFT_ENSEMBLE_MAX_CELLS");
+        if (e && *e) return (size_t)std::strtoull(e, nullptr, 10);
+        return (size_t)128 * 128 * 128;
+    }
+
+    int record_step(std::vector<LaunchRec> &out) override
+    {
+        if (int rc = tune()) return rc;
+        out.clear();
+        if (ncell >= ensemble_max_cells()) return HYDFT_E_UNSUPPORTED;
+        rec = &out;
+        rec_ok = true;
+        one_step();
+        rec = nullptr;
+        if (!rec_ok) {
+            out.clear();
+            return HYDFT_E_UNSUPPORTED;
+        }
+        return 0;
+    }
 
     void enqueue_steps(int k) override
     {
@@ -1596,14 +1733,84 @@ public:
         return 0;
     }
 
+    // The step's launches as an ensemble of one: the packs of one recorded
+    // step in this solver's device table, each launch the ensemble form
+    // with n = 1, so that the model alone and the same model in an ensemble
+    // group run the same compiled kernels (bit-identical fields).
+    // upload_recorded records one step and uploads its packs (synchronously,
+    // outside any capture); it returns false, with nothing uploaded, when a
+    // launch of the step has no ensemble form.
+    bool upload_recorded(std::vector<LaunchRec> &recs, std::vector<size_t> &off, int &rc)
+    {
+        rc = 0;
+        if (record_step(recs)) return false;
+        size_t total = 0;
+        off.assign(recs.size(), 0);
+        for (size_t i = 0; i < recs.size(); ++i) {
+            off[i] = total;
+            total += (recs[i].pack.size() + 255) / 256 * 256;
+        }
+        if (total > packcap) {
+            if (packbuf) cudaFree(packbuf);
+            packbuf = nullptr;
+            packcap = 0;
+            cudaError_t e = cudaMalloc(&packbuf, total);
+            if (e != cudaSuccess) { err = std::string("cudaMalloc: ") + cudaGetErrorString(e); rc = HYDFT_E_OOM; return true; }
+            packcap = total;
+        }
+        std::vector<unsigned char> host(total, 0);
+        for (size_t i = 0; i < recs.size(); ++i) std::memcpy(host.data() + off[i], recs[i].pack.data(), recs[i].pack.size());
+        cudaError_t e = cudaMemcpy(packbuf, host.data(), total, cudaMemcpyHostToDevice);
+        for (size_t i = 0; e == cudaSuccess && i < recs.size(); ++i) e = recs[i].prepare(recs[i].smem);
+        if (e != cudaSuccess) { err = std::string("pack table: ") + cudaGetErrorString(e); rc = HYDFT_E_CUDA; }
+        return true;
+    }
+
+    void launch_recorded(const std::vector<LaunchRec> &recs, const std::vector<size_t> &off)
+    {
+        for (size_t i = 0; i < recs.size(); ++i) {
+            const LaunchRec &r = recs[i];
+            cudaEvent_t ea = nullptr, eb = nullptr;
+            if (profiling) {
+                cudaEventCreate(&ea);
+                cudaEventCreate(&eb);
+                cudaEventRecord(ea, st);
+            }
+            r.launch(static_cast<unsigned char *>(packbuf) + off[i], 1, r.grid, r.block, r.smem, st);
+            launches++;
+            if (profiling) {
+                cudaEventRecord(eb, st);
+                int k = -1;
+                for (size_t j = 0; j < kstats.size(); ++j)
+                    if (kstats[j].name == r.name) k = (int)j;
+                if (k < 0) {
+                    kstats.push_back(KStat());
+                    kstats.back().name = r.name;
+                    k = (int)kstats.size() - 1;
+                }
+                kstats[k].bytes += r.bytes;
+                kstats[k].n += 1;
+                evrecs.push_back({k, ea, eb});
+            }
+        }
+    }
+
     int launch_steps(int nsteps) override
     {
         if (int rc = tune()) return rc;
         if (nsteps <= 0) return 0;
         if (!gexec) {
             const int64_t before = launches;
+            // the packs are uploaded before the capture begins
+            std::vector<LaunchRec> recs;
+            std::vector<size_t> off;
+            int rc = 0;
+            CK(cudaStreamSynchronize(st));
+            const bool ens = upload_recorded(recs, off, rc);
+            if (rc) return rc;
             CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-            one_step();
+            if (ens) launch_recorded(recs, off);
+            else one_step();
             cudaGraph_t gr = nullptr;
             CK(cudaStreamEndCapture(st, &gr));
             graph = gr;

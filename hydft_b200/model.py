@@ -138,6 +138,7 @@ def lib():
         L.hydft_batch_launch_count.argtypes = [_P]
         L.hydft_batch_stream.restype = _P
         L.hydft_batch_stream.argtypes = [_P]
+        L.hydft_batch_grouped.argtypes = [_P, C.POINTER(_I), C.POINTER(_I)]
         _lib = L
     return _lib
 
@@ -473,6 +474,13 @@ class Batch:
 
     def failed_member(self):
         return lib().hydft_batch_failed_member(self.b)
+
+    def grouped(self):
+        """(groups, members in groups) of the last captured ensemble step:
+        members in a group share every launch of the step."""
+        g, m = _I(), _I()
+        lib().hydft_batch_grouped(self.b, C.byref(g), C.byref(m))
+        return g.value, m.value
 
     def launch_count(self):
         return lib().hydft_batch_launch_count(self.b)

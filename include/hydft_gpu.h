@@ -257,7 +257,15 @@ int hydft_gpu_fd_alpha(int device, const double *y, double *alpha, int n);
  * the driver loop of src/hydft.f90:41-51; an ensemble holds many such
  * models (each with its own grid, species, Gamma, kappa and closure) on one
  * GPU and advances all of them by one RK3 step per launch of a single
- * captured CUDA graph in which every member is an independent branch.
+ * captured CUDA graph.  Members below 128^3 cells whose steps have the same
+ * launches (same grid, closure, precision and term kinds) form a group:
+ * each kernel of the step runs once for the whole group, every member's
+ * arguments read from a device table, so a group of 59 members of 48^3
+ * makes as many launches per step as one member.  Groups, members of 128^3
+ * cells or more (whose launches fill the GPU alone) and members whose step
+ * has no ensemble form (grids without register FFT plans) are independent
+ * branches of the graph.  A member's fields are bit-identical to the same
+ * model advanced alone.
  *
  * hydft_batch_create builds n members from params[i] (and structures[i]
  * when structures != NULL and structures[i].n > 0; members whose HNC
@@ -279,10 +287,13 @@ int hydft_batch_member(hydft_batch *b, int i, hydft_gpu **member);
 int hydft_batch_advance(hydft_batch *b, int nsteps);
 const char *hydft_batch_last_error(const hydft_batch *b);
 int hydft_batch_failed_member(const hydft_batch *b);
-/* kernels launched for all members so far, and the stream the ensemble
- * graph runs on (a cudaStream_t) */
+/* kernels the ensemble's graph launched so far (a group launch counts
+ * once), and the stream the ensemble graph runs on (a cudaStream_t) */
 int64_t hydft_batch_launch_count(const hydft_batch *b);
 void *hydft_batch_stream(const hydft_batch *b);
+/* groups of members stepped by shared launches, and the members in them,
+ * as of the last captured step (0 and 0 before the first advance) */
+int hydft_batch_grouped(const hydft_batch *b, int *groups, int *members);
 
 /* write_fields (src/model/io.f90:19-35): <prefix>_fld_NNNNNN.bin (NNNNNN =
  * step), raw little-endian: int32 nx, ny, nz, ndim, npi; float64 t, lx,

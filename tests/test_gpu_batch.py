@@ -22,6 +22,24 @@ MEMBERS = [
          lx=12.0, ly=6.0, lz=6.0, vext="driven", vext_amplitude=1e-3, vext_mode=(1, 0, 0), vext_omega=1.0, **HNC),
     dict(kind="ion", gamma=10.0, kappa=1.0, transport="yukawa_fit", nx=16, ny=16, nz=16,
          lx=10.0, ly=10.0, lz=10.0, gpu_precision="fp32", **HNC),
+    # grids with register FFT plans on every axis: members of equal shape
+    # step as one group (shared launches, per-member argument tables)
+    dict(kind="ion", gamma=5.0, kappa=0.5, transport="yukawa_fit", nx=32, ny=32, nz=32,
+         lx=20.0, ly=20.0, lz=20.0, gpu_precision="fp32", **HNC),
+    dict(kind="ion", gamma=40.0, kappa=2.5, transport="yukawa_fit", nx=32, ny=32, nz=32,
+         lx=20.0, ly=20.0, lz=20.0, gpu_precision="fp32", **HNC),
+    dict(kind="ion", gamma=20.0, kappa=1.5, closure="maxwell", transport="yukawa_fit", tau_model="ichimaru",
+         nx=48, ny=32, nz=32, lx=30.0, ly=20.0, lz=20.0, gpu_precision="fp32", **HNC),
+    dict(kind="ion", gamma=3.0, kappa=0.8, closure="maxwell", transport="yukawa_fit", tau_model="ichimaru",
+         nx=48, ny=32, nz=32, lx=24.0, ly=16.0, lz=16.0, gpu_precision="fp32", **HNC),
+    dict(kind="ion", gamma=8.0, kappa=1.0, transport="yukawa_fit", nx=32, ny=48, nz=64,
+         lx=16.0, ly=24.0, lz=32.0, **HNC),
+    dict(kind="electron", rs=1.0, theta=1.0, transport="constant", eta=0.2, nx=32, ny=32, nz=32,
+         lx=12.0, ly=12.0, lz=12.0, vext="driven", vext_amplitude=1e-3, vext_mode=(1, 0, 0), vext_omega=1.0,
+         gpu_precision="fp32", **HNC),
+    dict(kind="electron", rs=2.0, theta=0.5, transport="constant", eta=0.1, nx=32, ny=32, nz=32,
+         lx=12.0, ly=12.0, lz=12.0, vext="driven", vext_amplitude=1e-3, vext_mode=(1, 0, 0), vext_omega=0.7,
+         gpu_precision="fp32", **HNC),
 ]
 
 
@@ -51,6 +69,10 @@ def test_batch_matches_members_alone(hg):
             init(m, i)
         b.advance(3)
         b.advance(2)
+        # the 32^3 ion pair, the 48x32x32 Maxwell pair, the 32x48x64 member
+        # and the electron pair step in groups; the 16-point grids alone
+        groups, grouped = b.grouped()
+        assert groups >= 4 and grouped >= 7, (groups, grouped)
         for i, kw in enumerate(MEMBERS):
             alone = hg.Model(hg.default_params(**kw))
             init(alone, i)
