@@ -12,6 +12,7 @@
 
 #include "kernels.cuh"
 #include "regfft.cuh"
+#include "tma.cuh"
 
 namespace hydft {
 
@@ -207,7 +208,8 @@ struct ZinvPack {
 };
 
 template <typename R, int T, int E, int TX, int G, bool BAND>
-__device__ __forceinline__ void yinv_body(const BlockIx &bk, const Grid &g, const PassArgs<R> &a, const cplx<R> *twy)
+__device__ __forceinline__ void yinv_body(const BlockIx &bk, const Grid &g, const PassArgs<R> &a, const cplx<R> *twy,
+                                          const cplx<R> *tile = nullptr)
 {
     constexpr int L = T * E;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -218,7 +220,10 @@ __device__ __forceinline__ void yinv_body(const BlockIx &bk, const Grid &g, cons
     const bool valid = x < g.nkxc && z < g.nz;
     for (int i = tid; i < 2 * L; i += blockDim.x) tw[i] = twy[i];
     cplx<R> v[E];
-    load_band<R, T, E, BAND>(v, a.in[f] + (size_t)z * g.nkyc * g.pkx + x, g.pkx, t, g.My, g.nkyc, valid);
+    if (tile)   // the block's input tile, [G][nkyc][TX], loaded by TMA
+        load_band<R, T, E, BAND>(v, tile + (size_t)gi * g.nkyc * TX + c, TX, t, g.My, g.nkyc, valid);
+    else
+        load_band<R, T, E, BAND>(v, a.in[f] + (size_t)z * g.nkyc * g.pkx + x, g.pkx, t, g.My, g.nkyc, valid);
     // OP_IKY: the y derivative of a field whose z transform is shared with
     // other derivatives (k_y is constant along z); uniform over the block
     if (a.op[f] == OP_IKY) {
@@ -248,7 +253,8 @@ struct YinvPack {
 };
 
 template <typename R, int T, int E, int TX, int G, bool BAND>
-__device__ __forceinline__ void yfwd_body(const BlockIx &bk, const Grid &g, const PassArgs<R> &a, const cplx<R> *twy)
+__device__ __forceinline__ void yfwd_body(const BlockIx &bk, const Grid &g, const PassArgs<R> &a, const cplx<R> *twy,
+                                          const cplx<R> *tile = nullptr)
 {
     constexpr int L = T * E;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -259,7 +265,10 @@ __device__ __forceinline__ void yfwd_body(const BlockIx &bk, const Grid &g, cons
     const bool valid = x < g.nkxc && z < g.nz;
     for (int i = tid; i < 2 * L; i += blockDim.x) tw[i] = twy[i];
     cplx<R> v[E];
-    load_block<R, T, E>(v, a.in[f] + (size_t)z * g.ny * g.pkx + x, g.pkx, t, valid);
+    if (tile)   // the block's input tile, [G][ny][TX], loaded by TMA
+        load_block<R, T, E>(v, tile + (size_t)gi * g.ny * TX + c, TX, t, valid);
+    else
+        load_block<R, T, E>(v, a.in[f] + (size_t)z * g.ny * g.pkx + x, g.pkx, t, valid);
     __syncthreads();
     block_to_stride<T, E, -1, R, BarBlock, TX>(v, t, xb + gi * (L + L / T) * TX + c, tw);
     if (valid) store_band<R, T, E, BAND>(a.out[f] + (size_t)z * g.nkyc * g.pkx + x, v, g.pkx, t, g.My, g.nkyc, R(1));
@@ -281,7 +290,8 @@ struct YfwdPack {
 };
 
 template <typename R, int T, int E, int TX, int G, bool BAND, int NB>
-__device__ __forceinline__ void zfwd_body(const BlockIx &bk, const Grid &g, const PassArgs<R> &a, const cplx<R> *twz, R norm)
+__device__ __forceinline__ void zfwd_body(const BlockIx &bk, const Grid &g, const PassArgs<R> &a, const cplx<R> *twz, R norm,
+                                          const cplx<R> *tile = nullptr)
 {
     constexpr int L = T * E;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -296,7 +306,10 @@ __device__ __forceinline__ void zfwd_body(const BlockIx &bk, const Grid &g, cons
     for (int b = 0; b < NB; ++b) {
         const int kyc = (bk.y * NB + b) * G + gi;
         const bool valid = x < g.nkxc && kyc < g.nkyc;
-        load_block<R, T, E>(v[b], a.in[f] + (size_t)kyc * g.pkx + x, rs, t, valid);
+        if (tile)   // the block's input tile, [nz][G NB][TX], loaded by TMA
+            load_block<R, T, E>(v[b], tile + (size_t)(b * G + gi) * TX + c, G * NB * TX, t, valid);
+        else
+            load_block<R, T, E>(v[b], a.in[f] + (size_t)kyc * g.pkx + x, rs, t, valid);
     }
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
@@ -323,6 +336,92 @@ struct ZfwdPack {
     R norm;
     __device__ __forceinline__ void run(const BlockIx &b) const { zfwd_body<R, T, E, TX, G, BAND, NB>(b, g, a, tw, norm); }
 };
+
+// The TMA forms of the y inverse, y forward and z forward passes: thread 0
+// loads the block's whole input tile into the exchange buffer's space with
+// one tensor load (the tile is read into registers before the exchange
+// reuses that space), then the block runs the same body on the tile.  The
+// field coordinate of output f is src[f]; a wait that runs out sets
+// ST_TIMEOUT in *status and the block returns without storing.
+struct TmaFields {
+    int src[MAXF];
+    unsigned *status;
+};
+
+// The tile goes where the exchange buffer will be (after the 2L twiddles)
+// and its mbarrier right after the tile, inside the exchange buffer's
+// space too (the host checks tile + 8 bytes fit); the barrier is
+// invalidated before the body reuses that space.  Returns the tile, or
+// null when the destination is not 128-byte aligned (the block then reads
+// global memory as the plain pass does); ok is false when the wait ran out.
+template <typename R, int L>
+__device__ __forceinline__ cplx<R> *tma_tile_begin(const CUtensorMap *tm, int c0, int c1, int c2, int c3,
+                                                   unsigned bytes, bool &ok)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<R> *tile = reinterpret_cast<cplx<R> *>(smraw) + 2 * L;
+    unsigned long long *bar = reinterpret_cast<unsigned long long *>(reinterpret_cast<unsigned char *>(tile) + bytes);
+    ok = true;
+    if ((smem_u32(tile) & 127u) != 0) return nullptr;   // uniform over the block
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        mbar_expect_tx(bar, bytes);
+        tma_load_4d(tile, tm, c0, c1, c2, c3, bar);
+    }
+    __syncthreads();
+    ok = mbar_wait_bounded(bar, 0);
+    __syncthreads();
+    if (threadIdx.x == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+    return tile;
+}
+
+template <typename R, int T, int E, int TX, int G, bool BAND>
+__global__ void __launch_bounds__(TX * T * G) yinv_tma(const __grid_constant__ Grid g, const __grid_constant__ PassArgs<R> a,
+                                                      const cplx<R> *twy, const __grid_constant__ CUtensorMap tm,
+                                                      const __grid_constant__ TmaFields tf)
+{
+    const BlockIx bk = hw_block();
+    bool ok;
+    const cplx<R> *tile = tma_tile_begin<R, T * E>(&tm, 2 * TX * (int)bk.x, 0, G * (int)bk.y, tf.src[bk.z],
+                                                   (unsigned)(2 * TX * g.nkyc * G * sizeof(R)), ok);
+    if (!ok) {
+        if (threadIdx.x == 0) atomicOr(tf.status, ST_TIMEOUT);
+        return;
+    }
+    yinv_body<R, T, E, TX, G, BAND>(bk, g, a, twy, tile);
+}
+
+template <typename R, int T, int E, int TX, int G, bool BAND>
+__global__ void __launch_bounds__(TX * T * G) yfwd_tma(const __grid_constant__ Grid g, const __grid_constant__ PassArgs<R> a,
+                                                      const cplx<R> *twy, const __grid_constant__ CUtensorMap tm,
+                                                      const __grid_constant__ TmaFields tf)
+{
+    const BlockIx bk = hw_block();
+    bool ok;
+    const cplx<R> *tile = tma_tile_begin<R, T * E>(&tm, 2 * TX * (int)bk.x, 0, G * (int)bk.y, tf.src[bk.z],
+                                                   (unsigned)(2 * TX * g.ny * G * sizeof(R)), ok);
+    if (!ok) {
+        if (threadIdx.x == 0) atomicOr(tf.status, ST_TIMEOUT);
+        return;
+    }
+    yfwd_body<R, T, E, TX, G, BAND>(bk, g, a, twy, tile);
+}
+
+template <typename R, int T, int E, int TX, int G, bool BAND, int NB>
+__global__ void __launch_bounds__(TX * T * G) zfwd_tma(const __grid_constant__ Grid g, const __grid_constant__ PassArgs<R> a,
+                                                      const cplx<R> *twz, R norm, const __grid_constant__ CUtensorMap tm,
+                                                      const __grid_constant__ TmaFields tf)
+{
+    const BlockIx bk = hw_block();
+    bool ok;
+    const cplx<R> *tile = tma_tile_begin<R, T * E>(&tm, 2 * TX * (int)bk.x, G * NB * (int)bk.y, 0, tf.src[bk.z],
+                                                   (unsigned)(2 * TX * G * NB * g.nz * sizeof(R)), ok);
+    if (!ok) {
+        if (threadIdx.x == 0) atomicOr(tf.status, ST_TIMEOUT);
+        return;
+    }
+    zfwd_body<R, T, E, TX, G, BAND, NB>(bk, g, a, twz, norm, tile);
+}
 
 // smem bytes of a y/z fast pass
 template <typename R>

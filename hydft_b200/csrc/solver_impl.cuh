@@ -446,6 +446,21 @@ public:
     // forward one (HYDFT_ZNB_FWD=2 for two): at 256^3 two rows made the
     // inverse 10 % faster and the forward 4 % slower (same-box A/B)
     int z_nb = 2, z_nbf = 1;
+    // the y inverse, y forward and z forward passes of the plain path read
+    // each block's input tile with one TMA tensor load (HYDFT_TMA=0: every
+    // thread loads its own elements, as the ensemble forms always do; the
+    // fields are the same to the bit either way)
+    bool use_tma = true;
+
+    // field coordinates of the pass inputs in[0..nf-1] within the buffer
+    // base (fields `stride` complex values apart), for a TMA tensor map
+    TmaFields tma_fields(const cplx<R> *const *in, int nf, const cplx<R> *base, size_t stride)
+    {
+        TmaFields tf;
+        for (int f = 0; f < MAXF; ++f) tf.src[f] = f < nf ? (int)((in[f] - base) / (ptrdiff_t)stride) : 0;
+        tf.status = &ctrl->status;
+        return tf;
+    }
     // tile shapes picked by tune(): kx columns per y/z block, threads per x block
     int yz_tx = sizeof(R) == 4 ? 16 : 8;      // inverse y/z passes
     int yz_nt = sizeof(R) == 4 ? 256 : 128;
@@ -736,6 +751,8 @@ public:
             if (zn && std::string(zn) == "1") z_nb = 1;
             const char *znf = std::getenv("HYDFT_ZNB_FWD");
             if (znf && std::string(znf) == "2") z_nbf = 2;
+            const char *et = std::getenv("HYDFT_TMA");
+            if (et && std::string(et) == "0") use_tma = false;
             const char *eb = std::getenv("HYDFT_BAND");
             const bool band_ok = !(eb && std::string(eb) == "0");
             band_x = band_ok && g.Mx == (g.nx - 1) / 3;
@@ -901,13 +918,22 @@ public:
                 constexpr int G = yz_rows<T, TX, decltype(NTc)::value>();
                 const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
                 const dim3 grid((g.nkxc + TX - 1) / TX, (g.nz + G - 1) / G, nf);
-                auto go = [&](auto k, auto pk) {
+                auto go = [&](auto k, auto pk, auto kt) {
                     set_smem(k, sm);
                     pk.g = g; pk.a = b; pk.tw = tpy;
+                    const size_t tile = sizeof(cplx<R>) * (size_t)TX * g.nkyc * G;
+                    CUtensorMap tm;
+                    if (!rec && use_tma && tile + 8 <= sm - sizeof(cplx<R>) * 2 * T * E &&
+                        make_field_tmap<R>(&tm, zi, g.pkx, g.nkyc, g.nz, nin_max, TX, g.nkyc, G)) {
+                        const TmaFields tf = tma_fields(b.in, nf, zi, zsize);
+                        set_smem(kt, sm);
+                        launch("yinv", ybytes, [&] { kt<<<grid, TX * T * G, sm, st>>>(g, b, tpy, tm, tf); });
+                        return;
+                    }
                     launch_p("yinv", ybytes, grid, TX * T * G, sm, pk, [&] { k<<<grid, TX * T * G, sm, st>>>(g, b, tpy); });
                 };
-                if (band_y) go(yinv_fast<R, T, E, TX, G, true>, YinvPack<R, T, E, TX, G, true>{});
-                else go(yinv_fast<R, T, E, TX, G, false>, YinvPack<R, T, E, TX, G, false>{});
+                if (band_y) go(yinv_fast<R, T, E, TX, G, true>, YinvPack<R, T, E, TX, G, true>{}, yinv_tma<R, T, E, TX, G, true>);
+                else go(yinv_fast<R, T, E, TX, G, false>, YinvPack<R, T, E, TX, G, false>{}, yinv_tma<R, T, E, TX, G, false>);
             });
             });
             if (!yf) {
@@ -939,13 +965,22 @@ public:
                 constexpr int G = yz_rows<T, TX, decltype(NTc)::value>();
                 const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
                 const dim3 grid((g.nkxc + TX - 1) / TX, (g.nz + G - 1) / G, nf);
-                auto go = [&](auto k, auto pk) {
+                auto go = [&](auto k, auto pk, auto kt) {
                     set_smem(k, sm);
                     pk.g = g; pk.a = b; pk.tw = tpy;
+                    const size_t tile = sizeof(cplx<R>) * (size_t)TX * g.ny * G;
+                    CUtensorMap tm;
+                    if (!rec && use_tma && tile + 8 <= sm - sizeof(cplx<R>) * 2 * T * E &&
+                        make_field_tmap<R>(&tm, xo, g.pkx, g.ny, g.nz, nout_max, TX, g.ny, G)) {
+                        const TmaFields tf = tma_fields(b.in, nf, xo, ysize);
+                        set_smem(kt, sm);
+                        launch("yfwd", ybytes, [&] { kt<<<grid, TX * T * G, sm, st>>>(g, b, tpy, tm, tf); });
+                        return;
+                    }
                     launch_p("yfwd", ybytes, grid, TX * T * G, sm, pk, [&] { k<<<grid, TX * T * G, sm, st>>>(g, b, tpy); });
                 };
-                if (band_y) go(yfwd_fast<R, T, E, TX, G, true>, YfwdPack<R, T, E, TX, G, true>{});
-                else go(yfwd_fast<R, T, E, TX, G, false>, YfwdPack<R, T, E, TX, G, false>{});
+                if (band_y) go(yfwd_fast<R, T, E, TX, G, true>, YfwdPack<R, T, E, TX, G, true>{}, yfwd_tma<R, T, E, TX, G, true>);
+                else go(yfwd_fast<R, T, E, TX, G, false>, YfwdPack<R, T, E, TX, G, false>{}, yfwd_tma<R, T, E, TX, G, false>);
             });
             });
             if (!yf) {
@@ -969,18 +1004,27 @@ public:
             constexpr int TX = decltype(TXc)::value;
             constexpr int G = yz_rows<T, TX, decltype(NTc)::value>();
             const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
-            auto go = [&](auto k, auto pk, int nb) {
+            auto go = [&](auto k, auto pk, auto kt, int nb) {
                 set_smem(k, sm);
                 const dim3 grid((g.nkxc + TX - 1) / TX, (g.nkyc + G * nb - 1) / (G * nb), nf);
                 pk.g = g; pk.a = a; pk.tw = tpz; pk.norm = norm;
+                const size_t tile = sizeof(cplx<R>) * (size_t)TX * G * nb * g.nz;
+                CUtensorMap tm;
+                if (!rec && use_tma && src == zi && tile + 8 <= sm - sizeof(cplx<R>) * 2 * T * E &&
+                    make_field_tmap<R>(&tm, zi, g.pkx, g.nkyc, g.nz, nin_max, TX, G * nb, g.nz)) {
+                    const TmaFields tf = tma_fields(a.in, nf, zi, zsize);
+                    set_smem(kt, sm);
+                    launch("zfwd", zbytes, [&] { kt<<<grid, TX * T * G, sm, st>>>(g, a, tpz, norm, tm, tf); });
+                    return;
+                }
                 launch_p("zfwd", zbytes, grid, TX * T * G, sm, pk, [&] { k<<<grid, TX * T * G, sm, st>>>(g, a, tpz, norm); });
             };
             if (z_nbf == 2) {
-                if (band_z) go(zfwd_fast<R, T, E, TX, G, true, 2>, ZfwdPack<R, T, E, TX, G, true, 2>{}, 2);
-                else go(zfwd_fast<R, T, E, TX, G, false, 2>, ZfwdPack<R, T, E, TX, G, false, 2>{}, 2);
+                if (band_z) go(zfwd_fast<R, T, E, TX, G, true, 2>, ZfwdPack<R, T, E, TX, G, true, 2>{}, zfwd_tma<R, T, E, TX, G, true, 2>, 2);
+                else go(zfwd_fast<R, T, E, TX, G, false, 2>, ZfwdPack<R, T, E, TX, G, false, 2>{}, zfwd_tma<R, T, E, TX, G, false, 2>, 2);
             } else {
-                if (band_z) go(zfwd_fast<R, T, E, TX, G, true, 1>, ZfwdPack<R, T, E, TX, G, true, 1>{}, 1);
-                else go(zfwd_fast<R, T, E, TX, G, false, 1>, ZfwdPack<R, T, E, TX, G, false, 1>{}, 1);
+                if (band_z) go(zfwd_fast<R, T, E, TX, G, true, 1>, ZfwdPack<R, T, E, TX, G, true, 1>{}, zfwd_tma<R, T, E, TX, G, true, 1>, 1);
+                else go(zfwd_fast<R, T, E, TX, G, false, 1>, ZfwdPack<R, T, E, TX, G, false, 1>{}, zfwd_tma<R, T, E, TX, G, false, 1>, 1);
             }
             });
         });
