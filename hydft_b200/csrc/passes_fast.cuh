@@ -128,7 +128,8 @@ __device__ __forceinline__ void store_block(cplx<R> *__restrict__ col, const cpl
 // z passes: NB ky rows (G apart) per thread, all NB columns loaded before the
 // first is transformed, so that a thread keeps NB x E loads in flight
 template <typename R, int T, int E, int TX, int G, bool BAND, int NB>
-__device__ __forceinline__ void zinv_body(const BlockIx &bk, const Grid &g, const PassArgs<R> &a, const cplx<R> *twz)
+__device__ __forceinline__ void zinv_body(const BlockIx &bk, const Grid &g, const PassArgs<R> &a, const cplx<R> *twz,
+                                          const cplx<R> *tile = nullptr)
 {
     constexpr int L = T * E;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -147,7 +148,10 @@ __device__ __forceinline__ void zinv_body(const BlockIx &bk, const Grid &g, cons
     for (int b = 0; b < NB; ++b) {
         const int kyc = (bk.y * NB + b) * G + gi;
         const bool valid = x < g.nkxc && kyc < g.nkyc;
-        load_band<R, T, E, BAND>(v[b], a.in[f] + (size_t)kyc * g.pkx + x, rs, t, g.Mz, g.nkzc, valid);
+        if (tile)   // the block's input tile, [nkzc][G NB][TX], loaded by TMA
+            load_band<R, T, E, BAND>(v[b], tile + (size_t)(b * G + gi) * TX + c, G * NB * TX, t, g.Mz, g.nkzc, valid);
+        else
+            load_band<R, T, E, BAND>(v[b], a.in[f] + (size_t)kyc * g.pkx + x, rs, t, g.Mz, g.nkzc, valid);
     }
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
@@ -348,18 +352,19 @@ struct TmaFields {
     unsigned *status;
 };
 
-// The tile goes where the exchange buffer will be (after the 2L twiddles)
-// and its mbarrier right after the tile, inside the exchange buffer's
-// space too (the host checks tile + 8 bytes fit); the barrier is
+// The tile goes at complex offset `off`: where the exchange buffer will be
+// (after the 2L twiddles), or past the pass's own shared memory when it
+// does not fit there (z inverse); its mbarrier goes right after the tile
+// (the host sizes the space for tile + 8 bytes); the barrier is
 // invalidated before the body reuses that space.  Returns the tile, or
 // null when the destination is not 128-byte aligned (the block then reads
 // global memory as the plain pass does); ok is false when the wait ran out.
 template <typename R, int L>
 __device__ __forceinline__ cplx<R> *tma_tile_begin(const CUtensorMap *tm, int c0, int c1, int c2, int c3,
-                                                   unsigned bytes, bool &ok)
+                                                   unsigned bytes, bool &ok, size_t off = 2 * L)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
-    cplx<R> *tile = reinterpret_cast<cplx<R> *>(smraw) + 2 * L;
+    cplx<R> *tile = reinterpret_cast<cplx<R> *>(smraw) + off;
     unsigned long long *bar = reinterpret_cast<unsigned long long *>(reinterpret_cast<unsigned char *>(tile) + bytes);
     ok = true;
     if ((smem_u32(tile) & 127u) != 0) return nullptr;   // uniform over the block
@@ -369,10 +374,33 @@ __device__ __forceinline__ cplx<R> *tma_tile_begin(const CUtensorMap *tm, int c0
         tma_load_4d(tile, tm, c0, c1, c2, c3, bar);
     }
     __syncthreads();
-    ok = mbar_wait_bounded(bar, 0);
-    __syncthreads();
-    if (threadIdx.x == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+    // the block decides together, so that no thread leaves while others
+    // wait at a later barrier
+    ok = __syncthreads_and(mbar_wait_bounded(bar, 0)) != 0;
+    if (ok && threadIdx.x == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
     return tile;
+}
+
+// per-field tensor maps of the z inverse pass, whose inputs are separate
+// compact fields (map f covers in[f] alone)
+struct TmaMaps {
+    CUtensorMap m[16];
+};
+
+template <typename R, int T, int E, int TX, int G, bool BAND, int NB>
+__global__ void __launch_bounds__(TX * T * G) zinv_tma(const __grid_constant__ Grid g, const __grid_constant__ PassArgs<R> a,
+                                                      const cplx<R> *twz, const __grid_constant__ TmaMaps tm,
+                                                      unsigned tile_off, unsigned *status)
+{
+    const BlockIx bk = hw_block();
+    bool ok;
+    const cplx<R> *tile = tma_tile_begin<R, T * E>(&tm.m[bk.z], 2 * TX * (int)bk.x, G * NB * (int)bk.y, 0, 0,
+                                                   (unsigned)(2 * TX * G * NB * g.nkzc * sizeof(R)), ok, tile_off);
+    if (!ok) {
+        if (threadIdx.x == 0) atomicOr(status, ST_TIMEOUT);
+        return;
+    }
+    zinv_body<R, T, E, TX, G, BAND, NB>(bk, g, a, twz, tile);
 }
 
 template <typename R, int T, int E, int TX, int G, bool BAND>

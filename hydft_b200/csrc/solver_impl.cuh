@@ -881,18 +881,33 @@ public:
             constexpr int TX = decltype(TXc)::value;
             constexpr int G = yz_rows<T, TX, decltype(NTc)::value>();
             const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
-            auto go = [&](auto k, auto pk, int nb) {
+            auto go = [&](auto k, auto pk, auto kt, int nb) {
                 set_smem(k, sm);
                 const dim3 grid((g.nkxc + TX - 1) / TX, (g.nkyc + G * nb - 1) / (G * nb), nzf);
                 pk.g = g; pk.a = a; pk.tw = tpz;
+                // TMA: one map per input field; the tile goes past the pass's
+                // own shared memory (it does not fit in the exchange buffer)
+                const size_t tile = sizeof(cplx<R>) * (size_t)TX * G * nb * g.nkzc;
+                const size_t smt = (sm + tile + 8 + 127) / 128 * 128;
+                bool tma = !rec && use_tma && nzf <= 16 && sm % 128 == 0 && smt <= (size_t)smem_optin;
+                TmaMaps maps;
+                for (int f = 0; tma && f < nzf; ++f)
+                    tma = make_field_tmap<R>(&maps.m[f], a.in[f], g.pkx, g.nkyc, g.nkzc, 1, TX, G * nb, g.nkzc);
+                if (tma) {
+                    set_smem(kt, smt);
+                    const unsigned off = (unsigned)(sm / sizeof(cplx<R>));
+                    unsigned *stw = &ctrl->status;
+                    launch("zinv", zbytes, [&] { kt<<<grid, TX * T * G, smt, st>>>(g, a, tpz, maps, off, stw); });
+                    return;
+                }
                 launch_p("zinv", zbytes, grid, TX * T * G, sm, pk, [&] { k<<<grid, TX * T * G, sm, st>>>(g, a, tpz); });
             };
             if (z_nb == 2) {
-                if (band_z) go(zinv_fast<R, T, E, TX, G, true, 2>, ZinvPack<R, T, E, TX, G, true, 2>{}, 2);
-                else go(zinv_fast<R, T, E, TX, G, false, 2>, ZinvPack<R, T, E, TX, G, false, 2>{}, 2);
+                if (band_z) go(zinv_fast<R, T, E, TX, G, true, 2>, ZinvPack<R, T, E, TX, G, true, 2>{}, zinv_tma<R, T, E, TX, G, true, 2>, 2);
+                else go(zinv_fast<R, T, E, TX, G, false, 2>, ZinvPack<R, T, E, TX, G, false, 2>{}, zinv_tma<R, T, E, TX, G, false, 2>, 2);
             } else {
-                if (band_z) go(zinv_fast<R, T, E, TX, G, true, 1>, ZinvPack<R, T, E, TX, G, true, 1>{}, 1);
-                else go(zinv_fast<R, T, E, TX, G, false, 1>, ZinvPack<R, T, E, TX, G, false, 1>{}, 1);
+                if (band_z) go(zinv_fast<R, T, E, TX, G, true, 1>, ZinvPack<R, T, E, TX, G, true, 1>{}, zinv_tma<R, T, E, TX, G, true, 1>, 1);
+                else go(zinv_fast<R, T, E, TX, G, false, 1>, ZinvPack<R, T, E, TX, G, false, 1>{}, zinv_tma<R, T, E, TX, G, false, 1>, 1);
             }
             });
         });
