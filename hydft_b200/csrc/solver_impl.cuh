@@ -386,12 +386,32 @@ void ensemble_launch(const void *tab, unsigned n, dim3 grid, dim3 block, size_t 
     ensemble_kernel<P><<<dim3(grid.x, grid.y, grid.z * n), block, smem, st>>>(static_cast<const P *>(tab), grid.z);
 }
 
+// Raises a kernel's dynamic shared-memory limit to all that the current
+// device allows beside the kernel's static shared memory.  The limit only
+// caps what a launch may ask for (occupancy follows each launch's own
+// size), and it is never set lower: one kernel serves simulations whose
+// blocks differ in size (the tuner picks the threads per block for each
+// grid), and a limit fitted to one of them would make another's launch, or
+// a graph captured with it, invalid.  Fails when `need` does not fit.
+inline cudaError_t raise_smem_limit(const void *func, size_t need)
+{
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa;
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, func);
+    if (e != cudaSuccess) return e;
+    if ((size_t)optin < fa.sharedSizeBytes || need > (size_t)optin - fa.sharedSizeBytes) return cudaErrorInvalidValue;
+    if ((size_t)fa.maxDynamicSharedSizeBytes >= (size_t)optin - fa.sharedSizeBytes) return cudaSuccess;
+    return cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+}
+
 // the dynamic shared-memory limit of the ensemble form; its static copy of
 // the pack counts against the default 48 KB, so the limit is always set
 template <class P>
 cudaError_t ensemble_prepare(size_t smem)
 {
-    return cudaFuncSetAttribute(ensemble_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    return raise_smem_limit(reinterpret_cast<const void *>(&ensemble_kernel<P>), smem);
 }
 
 template <typename R>
@@ -842,7 +862,7 @@ public:
     template <class K>
     void set_smem(K k, size_t bytes)
     {
-        if (bytes > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (bytes > 48 * 1024) raise_smem_limit(reinterpret_cast<const void *>(k), bytes);
     }
 
     // inverse transform of nf spectral fields (with load-time operators) into
