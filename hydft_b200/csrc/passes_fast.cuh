@@ -18,6 +18,12 @@ namespace hydft {
 
 __device__ __forceinline__ int fft_signed(int n, int L) { return n <= L / 2 ? n : n - L; }
 
+// a b + c with one rounding, and a b rounded on its own (never contracted)
+__device__ __forceinline__ float fma_r(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_r(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+
 // ------------------------------------------------------------ y/z passes
 // Column element addressing with 32-bit offsets from a per-thread base: a
 // column of length L has its elements `rs` array elements apart.
@@ -486,11 +492,14 @@ __device__ __forceinline__ void x_c2r_load(cplx<R> (&v)[E], const cplx<R> *__res
     const cplx<R> zero = {R(0), R(0)};
     const R kxt = R(t) * kx0;
     // half-spectrum entries kk of a and b; kxk = kk kx0 for the derivative
+    // the derivative's products are rounded on their own (not contracted
+    // into the sums below), the same in every instantiation
+    auto ikx = [](R k, cplx<R> v) { return cplx<R>{mul_rn(-k, v.y), mul_rn(k, v.x)}; };
     auto get = [&](int kk, R kxk, cplx<R> &va, cplx<R> &vb) {
         va = ina[base + kk];
         vb = (BM == 1 || (BM == 2 && inb)) ? inb[base + kk] : zero;
-        if (dxa) va = ik_times(kxk, va);
-        if (dxb) vb = ik_times(kxk, vb);
+        if (dxa) va = ikx(kxk, va);
+        if (dxb) vb = ikx(kxk, vb);
     };
     // k = t + T e <= Mx: a_k + i b_k; k >= L - Mx: conj(a_{L-k}) + i conj(b_{L-k})
     auto lo = [&](int k, int e) {
@@ -812,30 +821,30 @@ struct XbFastPack {
     __device__ __forceinline__ void run(const BlockIx &b) const { xb_fast_body<R, T, E, NM, EVOLVE>(b, g, a, tw, pw); }
 };
 
-// 16-byte asynchronous global -> shared copies (cp.async, sm_80 and later);
-// the wait only covers this thread's own committed copies, so it ends.
-__device__ __forceinline__ void cp_async16(void *dst_smem, const void *src_gmem)
-{
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src_gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-// wait until at most one committed group of this thread is still in flight
-__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+// Staging of the x passes' input rows.  The rows of x a warp transforms
+// (32/T of them) are its own: lane 0 copies the warp's rows of each staged
+// field into shared memory with one bulk copy per field (the rows of a
+// block are contiguous in every field), completing on the warp's own
+// mbarrier, so no block-wide barrier follows the start of the pass.  The
+// barriers sit past the pass's other shared memory, 16 bytes per warp.
+template <int T>
+__host__ __device__ constexpr int x_rows_per_warp() { return 32 / T; }
 
-// cp.async of `rows` consecutive x rows of a spectral field (row stride pkx,
-// rows contiguous) starting at row0 into dst[rows][pkx]; every thread of the
-// block takes a share of the 16-byte chunks
-template <typename R>
-__device__ __forceinline__ void stage_rows(cplx<R> *dst, const cplx<R> *src, int row0, int rows, int pkx, int tid,
-                                           int nt)
+// the warp's rows that exist: inside its block (rb rows) and the grid
+template <int T>
+__device__ __forceinline__ int warp_rows(int w, int rb, int row0, int nrows)
 {
-    const int chunks = (int)((size_t)rows * pkx * sizeof(cplx<R>) / 16);
-    const char *s = reinterpret_cast<const char *>(src + (size_t)row0 * pkx);
-    char *d = reinterpret_cast<char *>(dst);
-    for (int i = tid; i < chunks; i += nt) cp_async16(d + 16 * (size_t)i, s + 16 * (size_t)i);
+    constexpr int RPW = x_rows_per_warp<T>();
+    return max(0, min(min(RPW, rb - w * RPW), nrows - row0 - w * RPW));
 }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Waits for phase `parity` of a warp's staging barrier.  A wait that runs
+// out (it is bounded) sets ST_TIMEOUT, which fails the step, and returns.
+__device__ __forceinline__ void warp_stage_wait(unsigned long long *bar, unsigned parity, unsigned *status)
+{
+    if (!mbar_wait_bounded(bar, parity) && (threadIdx.x & 31) == 0) atomicOr(status, ST_TIMEOUT);
+    __syncwarp();
+}
 
 // bulk prefetch of a 16-byte aligned global range (a multiple of 16 bytes)
 // into L2; no completion to wait for
@@ -865,6 +874,29 @@ struct XPrefetch {
     }
 };
 
+// row stride (elements) of the staged real rows: one row of x plus T, so
+// that the rows read by one warp start in different bank groups
+template <int T, int E>
+__host__ __device__ constexpr int xreal_stride() { return T * E + T; }
+
+// shared-memory bytes of the staged x passes before the warps' staging
+// barriers: twiddles, staged spectral rows (nstage fields), exchange rows,
+// staged real rows (nreal fields), rounded up to 16
+template <typename R, int T, int E>
+__host__ __device__ inline size_t xstaged_body_bytes(int nt, int pkx, int nstage, int nreal)
+{
+    const int rb = nt / T;
+    const size_t b = sizeof(cplx<R>) * (2 * (size_t)T * E + (size_t)nstage * rb * pkx + (size_t)rb * xrow_stride<T, E>()) +
+                     sizeof(R) * (size_t)nreal * rb * xreal_stride<T, E>();
+    return (b + 15) / 16 * 16;
+}
+// all of it: two 8-byte barriers per warp after the body
+template <typename R, int T, int E>
+inline size_t xstaged_smem(int nt, int pkx, int nstage, int nreal)
+{
+    return xstaged_body_bytes<R, T, E>(nt, pkx, nstage, nreal) + 16 * (size_t)((nt + 31) / 32);
+}
+
 // blocks per SM the staged x passes are compiled for: two 256-thread blocks
 // in single precision with up to 16 values per thread, else one
 template <typename R, int E>
@@ -874,7 +906,8 @@ __host__ __device__ constexpr int xstaged_minb() { return sizeof(R) == 4 && E <=
 // relaxation finish): the four inputs dn, m_0..m_2 stay in registers as two
 // pairs, so no per-thread shared-memory slots are needed and two 256-thread
 // blocks fit on an SM.  The block's spectral input rows are copied into
-// shared memory by cp.async first.  The output pairs are ordered so that dn is consumed
+// shared memory first (each warp its own rows, by bulk copies: pair 1
+// lands while pair 0 is transformed).  The output pairs are ordered so that dn is consumed
 // first: (mu_local, u_0), (u_1, u_2), (m0u0, m0u1), (m0u2, m1u1), (m1u2, m2u2);
 // UONLY: (u_0, u_1), (u_2, -).  Outputs go to the same fields as xa_fast's.
 template <typename R, int T, int E, bool UONLY, bool BAND>
@@ -890,23 +923,35 @@ __device__ __forceinline__ void xa_regs_body(const BlockIx &bk, const Grid &g, c
     const int tid = threadIdx.x, t = tid % T, rr = tid / T;
     const int row0 = bk.x * rb, row = row0 + rr;
     const bool rowok = row < g.ny * g.nz;
-    const int vrows = max(0, min(rb, g.ny * g.nz - row0));
     cplx<R> *xrow = xbuf + rr * xrow_stride<T, E>();
-    // the block's rows of all four inputs on their way at once, one commit
-    // group per pair: pair 1 lands while pair 0 is transformed
-    for (int f = 0; f < 4; ++f) {
-        stage_rows(sb + (size_t)f * rb * pk, a.in[f], row0, vrows, pk, tid, nt);
-        if (f & 1) cp_async_commit();
+    // the warp's rows of all four inputs on their way at once, one barrier
+    // per pair: pair 1 lands while pair 0 is transformed
+    constexpr int RPW = x_rows_per_warp<T>();
+    const int lane = tid & 31, w = tid >> 5;
+    const int wrows = warp_rows<T>(w, rb, row0, g.ny * g.nz);
+    unsigned long long *bars =
+        reinterpret_cast<unsigned long long *>(smraw + xstaged_body_bytes<R, T, E>(nt, pk, 4, 0)) + 2 * w;
+    if (lane == 0) {
+        mbar_init(bars, 1);
+        mbar_init(bars + 1, 1);
+        if (wrows > 0) {
+            const unsigned bytes = (unsigned)(wrows * pk * sizeof(cplx<R>));
+            const size_t src = (size_t)(row0 + w * RPW) * pk;
+            for (int q = 0; q < 2; ++q) {
+                mbar_expect_tx(bars + q, 2 * bytes);
+                for (int f = 2 * q; f < 2 * q + 2; ++f)
+                    bulk_load(sb + ((size_t)f * rb + w * RPW) * pk, a.in[f] + src, bytes, bars + q);
+            }
+        }
     }
     for (int i = tid; i < 2 * L; i += nt) tw[i] = twx[i];
+    __syncthreads();
     cplx<R> p0[E], p1[E];   // (dn, m_0), (m_1, m_2)
     const size_t sbase = (size_t)rr * pk;
-    cp_async_wait_one();
-    __syncthreads();
+    if (wrows > 0) warp_stage_wait(bars, 0, pw.status);
     x_c2r_load<R, T, E, BAND, 1>(p0, sb, sb + (size_t)rb * pk, sbase, true, t, g.Mx);
     stride_to_block<T, E, +1, R, BarWarp, 1>(p0, t, xrow, tw);
-    cp_async_wait_all();
-    __syncthreads();
+    if (wrows > 0) warp_stage_wait(bars + 1, 0, pw.status);
     x_c2r_load<R, T, E, BAND, 1>(p1, sb + 2 * (size_t)rb * pk, sb + 3 * (size_t)rb * pk, sbase, true, t, g.Mx);
     stride_to_block<T, E, +1, R, BarWarp, 1>(p1, t, xrow, tw);
     const double nref64 = *pw.nmean;
@@ -996,15 +1041,12 @@ struct XaRegsPack {
     __device__ __forceinline__ void run(const BlockIx &b) const { xa_regs_body<R, T, E, UONLY, BAND>(b, g, a, tw, pw); }
 };
 
-// row stride (elements) of the staged real rows: one row of x plus T, so
-// that the rows read by one warp start in different bank groups
-template <int T, int E>
-__host__ __device__ constexpr int xreal_stride() { return T * E + T; }
-
-// Phase B with this block's real-space rows (dn and, when Pi evolves, u_d)
-// copied into shared memory by cp.async at the start; the copies overlap the
-// first inverse transform, and the spectral inputs are prefetched to L2 a few
-// fields ahead.  Same inputs, outputs and arithmetic as xb_fast, except that
+// Phase B with each warp's real-space u_d rows (when Pi evolves) copied into
+// shared memory at the start with the first input pair, and each input pair
+// staged one pair ahead of the transform that reads it (bulk copies on the
+// warp's own barrier, whose phases follow the pairs); the spectral inputs
+// are prefetched to L2 a few fields ahead and dn comes straight into
+// registers.  Same inputs, outputs and arithmetic as xb_fast, except that
 // with a.dx_in_pass the x derivatives (of mu and of each Pi component)
 // arrive underived, sharing their z and y transforms with the y derivative,
 // and are differentiated here on the way in.  EXTK: no external force (0), a
@@ -1015,8 +1057,7 @@ __device__ __forceinline__ void xb_rows_body(const BlockIx &bk, const Grid &g, c
 {
     constexpr int L = T * E, NM = 3;
     constexpr int RS = xreal_stride<T, E>();
-    constexpr int CPR = L * (int)sizeof(R) / 16;   // 16-byte chunks per real row
-    constexpr int EPC = 16 / (int)sizeof(R);        // elements per chunk
+    constexpr int RPW = x_rows_per_warp<T>();
     constexpr int AHEAD = 6;                        // fields prefetched to L2 ahead
     constexpr int NPAIR = EVOLVE ? 2 + 3 * NM : 2;  // (dmu_0, dmu_1), (dmu_2), (dPi pairs)
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -1033,37 +1074,49 @@ __device__ __forceinline__ void xb_rows_body(const BlockIx &bk, const Grid &g, c
     cplx<R> *xrow = xbuf + rr * xrow_stride<T, E>();
     const int vrows = max(0, min(rb, nrows - row0));
     const size_t rowbase = (size_t)row * L;
+    const int lane = tid & 31, w = tid >> 5, wr0 = w * RPW;
+    const int wrows = warp_rows<T>(w, rb, row0, nrows);
+    unsigned long long *bar = reinterpret_cast<unsigned long long *>(
+                                  smraw + xstaged_body_bytes<R, T, E>(nt, pk, 2, EVOLVE ? NM : 0)) + 2 * w;
+    unsigned phase = 0;
     // fields of pair p: (0, 1), (2, -), then (3 + 2q, 4 + 2q)
     auto fields = [&](int p, int &fa, int &fb) {
         if (p == 0) { fa = 0; fb = 1; }
         else if (p == 1) { fa = 2; fb = -1; }
         else { fa = NM + 2 * (p - 2); fb = fa + 1; }
     };
+    // the warp's rows of pair p (and with pair 0 its u rows) on their way;
+    // the lanes have read the previous pair from the same space (the caller
+    // synchronises the warp), hence the proxy fence
     auto stage = [&](int p) {
-        if (p >= NPAIR) return;
+        if (p >= NPAIR || lane != 0 || wrows == 0) return;
         int fa, fb;
         fields(p, fa, fb);
-        stage_rows(sb, a.in[fa], row0, vrows, pk, tid, nt);
-        if (fb >= 0) stage_rows(sb + (size_t)rb * pk, a.in[fb], row0, vrows, pk, tid, nt);
-        cp_async_commit();
+        const unsigned bytes = (unsigned)(wrows * pk * sizeof(cplx<R>));
+        const unsigned ubytes = (unsigned)(L * sizeof(R));
+        unsigned total = bytes * (fb >= 0 ? 2u : 1u);
+        if (EVOLVE && p == 0) total += NM * wrows * ubytes;
+        fence_proxy_async_shared();
+        mbar_expect_tx(bar, total);
+        const size_t src = (size_t)(row0 + wr0) * pk;
+        bulk_load(sb + (size_t)wr0 * pk, a.in[fa] + src, bytes, bar);
+        if (fb >= 0) bulk_load(sb + (size_t)(rb + wr0) * pk, a.in[fb] + src, bytes, bar);
+        if (EVOLVE && p == 0)
+            for (int f = 0; f < NM; ++f)
+                for (int j = 0; j < wrows; ++j)
+                    bulk_load(rs + ((size_t)f * rb + wr0 + j) * RS,
+                              pw.u_real + (size_t)f * pw.ncell + (size_t)(row0 + wr0 + j) * L, ubytes, bar);
     };
-    // pair 0 and the u rows on their way; dn from global into registers
+    if (lane == 0) mbar_init(bar, 1);
+    __syncwarp();
     stage(0);
-    if (EVOLVE) {
-        const int total = NM * vrows * CPR;
-        for (int i = tid; i < total; i += nt) {
-            const int c = i % CPR, j = (i / CPR) % vrows, f = i / (CPR * vrows);
-            const R *src = pw.u_real + (size_t)f * pw.ncell + (size_t)(row0 + j) * L + c * EPC;
-            cp_async16(rs + ((size_t)f * rb + j) * RS + c * EPC, src);
-        }
-        cp_async_commit();
-    }
     XPrefetch<R> pf(a, g, row0, vrows, tid == 0);
     pf.upto(AHEAD);
     R dnv[E];
 #pragma unroll
     for (int r = 0; r < E; ++r) dnv[r] = rowok ? pw.dn_real[rowbase + block_pos<T, E>(t, r)] : R(0);
     for (int i = tid; i < 2 * L; i += nt) tw[i] = twx[i];
+    __syncthreads();
     // the staged pair p into registers, then pair p + 1 on its way
     const R kx0 = R(g.kx0);
     const bool dxs = a.dx_in_pass != 0;
@@ -1073,11 +1126,13 @@ __device__ __forceinline__ void xb_rows_body(const BlockIx &bk, const Grid &g, c
         constexpr int BM = decltype(bm)::value;
         int fa, fb;
         fields(p, fa, fb);
-        cp_async_wait_all();
-        __syncthreads();
+        if (wrows > 0) {
+            warp_stage_wait(bar, phase, pw.status);
+            phase ^= 1u;
+        }
         x_c2r_load<R, T, E, BAND, BM>(v, sb, BM ? sb + (size_t)rb * pk : nullptr, (size_t)rr * pk, true, t, g.Mx,
                                       dxa, dxb, kx0);
-        __syncthreads();
+        __syncwarp();
         stage(p + 1);
         pf.upto((fb >= 0 ? fb : fa) + 2 + AHEAD);
     };
@@ -1128,7 +1183,12 @@ __device__ __forceinline__ void xb_rows_body(const BlockIx &bk, const Grid &g, c
                 stride_to_block<T, E, +1, R, BarWarp, 1>(v, t, xrow, tw);
                 const R *urow = rs + ((size_t)d * rb + rr) * RS;
 #pragma unroll
-                for (int r = 0; r < E; ++r) acc[r] = acc[r] - urow[block_pos<T, E>(t, r)] * v[r];
+                for (int r = 0; r < E; ++r) {
+                    // explicit fused multiply-adds: the rounding does not depend
+                    // on how the compiler contracts this instantiation
+                    const R u = urow[block_pos<T, E>(t, r)];
+                    acc[r] = cplx<R>{fma_r(-u, v[r].x, acc[r].x), fma_r(-u, v[r].y, acc[r].y)};
+                }
             }
             x_r2c_pair<R, T, E, BAND, 1, true>(acc, a.out[NM + 2 * cp], a.out[NM + 2 * cp + 1], row, rowok, t, g,
                                                xrow, tw);
@@ -1153,15 +1213,6 @@ struct XbRowsPack {
     __device__ __forceinline__ void run(const BlockIx &b) const { xb_rows_body<R, T, E, EVOLVE, EXTK, BAND>(b, g, a, tw, pw); }
 };
 
-// shared-memory bytes of the staged x passes: twiddles, staged spectral
-// rows (nstage fields), exchange rows, staged real rows (nreal fields)
-template <typename R, int T, int E>
-inline size_t xstaged_smem(int nt, int pkx, int nstage, int nreal)
-{
-    const int rb = nt / T;
-    return sizeof(cplx<R>) * (2 * (size_t)T * E + (size_t)nstage * rb * pkx + (size_t)rb * xrow_stride<T, E>()) +
-           sizeof(R) * (size_t)nreal * rb * xreal_stride<T, E>();
-}
 
 
 // Real-space I/O: half spectra -> real fields (TOREAL) or back.

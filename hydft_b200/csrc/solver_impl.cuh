@@ -471,6 +471,7 @@ public:
     // thread loads its own elements, as the ensemble forms always do; the
     // fields are the same to the bit either way)
     bool use_tma = true;
+    bool tma_zinv = true;        // the z inverse pass's TMA form (HYDFT_TMA_ZINV=0 switches it off)
 
     // field coordinates of the pass inputs in[0..nf-1] within the buffer
     // base (fields `stride` complex values apart), for a TMA tensor map
@@ -773,6 +774,8 @@ public:
             if (znf && std::string(znf) == "2") z_nbf = 2;
             const char *et = std::getenv("HYDFT_TMA");
             if (et && std::string(et) == "0") use_tma = false;
+            const char *ez = std::getenv("HYDFT_TMA_ZINV");
+            if (ez) tma_zinv = std::string(ez) != "0";
             const char *eb = std::getenv("HYDFT_BAND");
             const bool band_ok = !(eb && std::string(eb) == "0");
             band_x = band_ok && g.Mx == (g.nx - 1) / 3;
@@ -909,7 +912,7 @@ public:
                 // own shared memory (it does not fit in the exchange buffer)
                 const size_t tile = sizeof(cplx<R>) * (size_t)TX * G * nb * g.nkzc;
                 const size_t smt = (sm + tile + 8 + 127) / 128 * 128;
-                bool tma = !rec && use_tma && nzf <= 16 && sm % 128 == 0 && smt <= (size_t)smem_optin;
+                bool tma = !rec && use_tma && tma_zinv && nzf <= 16 && sm % 128 == 0 && smt <= (size_t)smem_optin;
                 TmaMaps maps;
                 for (int f = 0; tma && f < nzf; ++f)
                     tma = make_field_tmap<R>(&maps.m[f], a.in[f], g.pkx, g.nkyc, g.nkzc, 1, TX, G * nb, g.nkzc);
@@ -1123,7 +1126,7 @@ public:
                 // of shared memory per SM, 1 KB reserved per block, and the
                 // ensemble form's copy of its pack
                 const size_t cap = (xstaged_minb<R, E>() == 2 ? 115712 : (size_t)smem_optin) - sizeof(pk);
-                while (sm > cap && nt > T) {
+                while (sm > cap && nt > 32) {   // whole warps: each stages its own rows
                     nt /= 2;
                     sm = xstaged_smem<R, T, E>(nt, g.pkx, 4, 0);
                 }
@@ -1171,7 +1174,7 @@ public:
                 size_t sm = xstaged_smem<R, T, E>(nt, g.pkx, 2, nreal_rows);
                 // two blocks per SM: 228 KB of shared memory, 1 KB reserved per
                 // block, and the ensemble form's copy of its pack
-                while (sm > 115712 - sizeof(pk) && nt > T) {
+                while (sm > 115712 - sizeof(pk) && nt > 32) {   // whole warps
                     nt /= 2;
                     sm = xstaged_smem<R, T, E>(nt, g.pkx, 2, nreal_rows);
                 }

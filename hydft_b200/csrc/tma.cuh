@@ -121,4 +121,19 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *tm, in
         : "memory");
 }
 
+// One untiled bulk copy of `bytes` (a multiple of 16) from global memory
+// into this CTA's shared memory, completing on bar; both addresses 16-byte
+// aligned; no multicast, and the source is this GPU's memory.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, unsigned long long *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// Orders this thread's earlier shared-memory accesses (and those ordered
+// before them by a barrier) before later bulk copies into the same space.
+__device__ __forceinline__ void fence_proxy_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
 }  // namespace hydft
