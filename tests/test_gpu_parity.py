@@ -369,13 +369,15 @@ def test_tile_shapes_give_identical_results(hg, monkeypatch):
 def test_tma_tile_loads_give_identical_results(hg, monkeypatch, prec):
     """The y inverse, y forward and z forward passes of a 128^3 model (which
     steps with the plain kernels) read their input tiles with TMA tensor
-    loads; with HYDFT_TMA=0 every thread loads its own elements.  Same
-    fields to the bit, after steps and in the right-hand side."""
+    loads, and with HYDFT_TMA_ZINV=1 the z inverse pass too; with
+    HYDFT_TMA=0 every thread loads its own elements.  Same fields to the
+    bit, after steps and in the right-hand side."""
     kw = dict(ION, nx=128, ny=128, nz=128, lx=64.0, ly=64.0, lz=64.0, closure="maxwell", tau_model="constant",
               tau=1.5, dt=0.01, gpu_precision=prec)
     out = []
     for flag in ("0", "1"):
         monkeypatch.setenv("HYDFT_TMA", flag)
+        monkeypatch.setenv("HYDFT_TMA_ZINV", flag)
         m = hg.Model(hg.default_params(**kw))
         n, mom, pi = seeded_state(m, seed=9)
         m.set_state(n, mom, pi)
@@ -384,6 +386,7 @@ def test_tma_tile_loads_give_identical_results(hg, monkeypatch, prec):
         out.append(list(m.get_state()) + list(r))
         m.close()
     monkeypatch.delenv("HYDFT_TMA")
+    monkeypatch.delenv("HYDFT_TMA_ZINV")
     for x, y in zip(out[0], out[1]):
         if x is not None:
             assert np.array_equal(x, y)
