@@ -874,10 +874,12 @@ struct XPrefetch {
     }
 };
 
-// row stride (elements) of the staged real rows: one row of x plus T, so
-// that the rows read by one warp start in different bank groups
+// Staged real rows: each row of x holds its nreal fields back to back (one
+// row of x each), and rows are nreal L + T elements apart, so that the rows
+// read by one warp start T banks apart (L is a multiple of 16, and of 32
+// where T > 4) and never collide
 template <int T, int E>
-__host__ __device__ constexpr int xreal_stride() { return T * E + T; }
+__host__ __device__ constexpr int xreal_stride(int nreal) { return nreal * T * E + T; }
 
 // shared-memory bytes of the staged x passes before the warps' staging
 // barriers: twiddles, staged spectral rows (nstage fields), exchange rows,
@@ -887,7 +889,7 @@ __host__ __device__ inline size_t xstaged_body_bytes(int nt, int pkx, int nstage
 {
     const int rb = nt / T;
     const size_t b = sizeof(cplx<R>) * (2 * (size_t)T * E + (size_t)nstage * rb * pkx + (size_t)rb * xrow_stride<T, E>()) +
-                     sizeof(R) * (size_t)nreal * rb * xreal_stride<T, E>();
+                     (nreal ? sizeof(R) * (size_t)rb * xreal_stride<T, E>(nreal) : 0);
     return (b + 15) / 16 * 16;
 }
 // all of it: two 8-byte barriers per warp after the body
@@ -1056,7 +1058,7 @@ __device__ __forceinline__ void xb_rows_body(const BlockIx &bk, const Grid &g, c
     const cplx<R> *twx, const PWB<R> &pw)
 {
     constexpr int L = T * E, NM = 3;
-    constexpr int RS = xreal_stride<T, E>();
+    constexpr int RS = xreal_stride<T, E>(NM);
     constexpr int RPW = x_rows_per_warp<T>();
     constexpr int AHEAD = 6;                        // fields prefetched to L2 ahead
     constexpr int NPAIR = EVOLVE ? 2 + 3 * NM : 2;  // (dmu_0, dmu_1), (dmu_2), (dPi pairs)
@@ -1065,7 +1067,7 @@ __device__ __forceinline__ void xb_rows_body(const BlockIx &bk, const Grid &g, c
     const int nt = blockDim.x, rb = nt / T, pk = g.pkx;
     cplx<R> *sb = tw + 2 * L;                       // [2][rb][pkx] the staged input pair
     cplx<R> *xbuf = sb + 2 * (size_t)rb * pk;
-    R *rs = reinterpret_cast<R *>(xbuf + rb * xrow_stride<T, E>());   // [3][rb][RS] u rows
+    R *rs = reinterpret_cast<R *>(xbuf + rb * xrow_stride<T, E>());   // [rb][RS]: u rows, 3 per row of x
     const int tid = threadIdx.x, t = tid % T, rr = tid / T;
     const int nrows = g.ny * g.nz;
     const int row0 = bk.x * rb;
@@ -1104,7 +1106,7 @@ __device__ __forceinline__ void xb_rows_body(const BlockIx &bk, const Grid &g, c
         if (EVOLVE && p == 0)
             for (int f = 0; f < NM; ++f)
                 for (int j = 0; j < wrows; ++j)
-                    bulk_load(rs + ((size_t)f * rb + wr0 + j) * RS,
+                    bulk_load(rs + (size_t)(wr0 + j) * RS + f * L,
                               pw.u_real + (size_t)f * pw.ncell + (size_t)(row0 + wr0 + j) * L, ubytes, bar);
     };
     if (lane == 0) mbar_init(bar, 1);
@@ -1181,7 +1183,7 @@ __device__ __forceinline__ void xb_rows_body(const BlockIx &bk, const Grid &g, c
                 cplx<R> v[E];
                 load(2 + cp * NM + d, v, dxs && d == 0, dxs && d == 0, B1{});   // d/dx of Pi
                 stride_to_block<T, E, +1, R, BarWarp, 1>(v, t, xrow, tw);
-                const R *urow = rs + ((size_t)d * rb + rr) * RS;
+                const R *urow = rs + (size_t)rr * RS + d * L;
 #pragma unroll
                 for (int r = 0; r < E; ++r) {
                     // explicit fused multiply-adds: the rounding does not depend
