@@ -29,11 +29,12 @@ using namespace hydft;
 
 // Members whose steps record the same launches (kernel kinds and shapes)
 // step together: each launch of the step runs once for the whole group, on
-// the group's stream, with the members' arguments in a device table.
+// the group's stream, with the members' arguments (packs) as kernel
+// parameters.
 struct EnsembleGroup {
     std::vector<int> members;
     std::vector<LaunchRec> recs;     // the first member's launches (kinds and shapes)
-    std::vector<size_t> tab_off;     // offset of each launch's pack table in the table buffer
+    std::vector<std::vector<unsigned char>> packs;   // per launch: the members' packs back to back
     cudaStream_t st = nullptr;
     cudaEvent_t done = nullptr;
 };
@@ -49,7 +50,6 @@ struct hydft_batch {
     std::vector<int64_t> step_launches;  // kernels of one member step, as the member alone would launch them
     std::vector<EnsembleGroup> groups;
     std::vector<int> solo;               // members stepping on their own stream (no ensemble form)
-    void *dtab = nullptr;                // the groups' pack tables (device)
     int64_t graph_kernels = 0;           // kernels per graph launch
     int64_t launches = 0;                // kernels launched by this ensemble's graph so far
     unsigned *hstat = nullptr;           // pinned status words, one per member
@@ -99,8 +99,6 @@ void drop_groups(hydft_batch *b)
     }
     b->groups.clear();
     b->solo.clear();
-    if (b->dtab) cudaFree(b->dtab);
-    b->dtab = nullptr;
 }
 
 void drop_graph(hydft_batch *b)
@@ -123,7 +121,7 @@ std::string step_signature(const std::vector<LaunchRec> &recs)
 }
 
 // Records every member's step, groups members with the same launches and
-// builds their pack tables; members without an ensemble form step alone.
+// gathers their packs; members without an ensemble form step alone.
 int build_groups(hydft_batch *b)
 {
     drop_groups(b);
@@ -147,26 +145,15 @@ int build_groups(hydft_batch *b)
         }
         b->groups[it->second].members.push_back((int)i);
     }
-    // one table per launch per group: the members' packs back to back
-    size_t total = 0;
+    // per launch per group: the members' packs back to back
     for (auto &g : b->groups) {
-        g.tab_off.resize(g.recs.size());
+        g.packs.resize(g.recs.size());
         for (size_t r = 0; r < g.recs.size(); ++r) {
-            g.tab_off[r] = total;
-            total += (g.recs[r].pack.size() * g.members.size() + 255) / 256 * 256;
+            const size_t sz = g.recs[r].pack.size();
+            g.packs[r].assign(sz * g.members.size(), 0);
+            for (size_t j = 0; j < g.members.size(); ++j)
+                std::memcpy(g.packs[r].data() + j * sz, recs[g.members[j]][r].pack.data(), sz);
         }
-    }
-    if (total) {
-        std::vector<unsigned char> host(total, 0);
-        for (auto &g : b->groups)
-            for (size_t r = 0; r < g.recs.size(); ++r) {
-                const size_t sz = g.recs[r].pack.size();
-                for (size_t j = 0; j < g.members.size(); ++j)
-                    std::memcpy(host.data() + g.tab_off[r] + j * sz, recs[g.members[j]][r].pack.data(), sz);
-            }
-        if (cudaMalloc(&b->dtab, total) != cudaSuccess) return fail(b, HYDFT_ERR_OOM, "ensemble: pack tables");
-        cudaError_t e = cudaMemcpy(b->dtab, host.data(), total, cudaMemcpyHostToDevice);
-        if (e != cudaSuccess) return fail(b, HYDFT_ERR_CUDA, std::string("ensemble: pack tables: ") + cudaGetErrorString(e));
     }
     for (auto &g : b->groups) {
         if (cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking) != cudaSuccess ||
@@ -200,8 +187,7 @@ int capture(hydft_batch *b)
         cudaStreamWaitEvent(g.st, b->fork, 0);
         for (size_t r = 0; r < g.recs.size(); ++r) {
             const LaunchRec &lr = g.recs[r];
-            lr.launch(static_cast<unsigned char *>(b->dtab) + g.tab_off[r], (unsigned)g.members.size(), lr.grid, lr.block,
-                      lr.smem, g.st);
+            lr.launch(g.packs[r].data(), (unsigned)g.members.size(), lr.grid, lr.block, lr.smem, g.st);
             const cudaError_t le = cudaGetLastError();
             if (le != cudaSuccess) {
                 cudaGraph_t dead = nullptr;
@@ -214,7 +200,8 @@ int capture(hydft_batch *b)
                 return fail(b, HYDFT_ERR_CUDA, buf + std::string(cudaGetErrorString(le)));
             }
         }
-        kernels += (int64_t)g.recs.size();
+        for (const LaunchRec &lr : g.recs)
+            kernels += (int64_t)((g.members.size() + lr.per_launch - 1) / lr.per_launch);
         cudaEventRecord(g.done, g.st);
         cudaStreamWaitEvent(b->root, g.done, 0);
     }

@@ -89,23 +89,28 @@ __device__ __forceinline__ BlockIx hw_block()
 
 // The ensemble form of a kernel.  P (a "pack") holds one simulation's
 // launch arguments and runs the kernel body for one block of that
-// simulation's grid; tab[m] is simulation m's pack (in device memory) and
-// zper the z extent of one simulation's grid, so block z = m zper + z'.
-// Each block first copies its simulation's pack into shared memory: the
-// body then reads its arguments from an address space that its global
-// stores cannot alias, so they are loaded once rather than after every
-// store.  A model on its own runs the same kernel with one pack.
+// simulation's grid.  The packs of up to PackSet<P>::N simulations travel as
+// one kernel parameter (__grid_constant__, under the 32 KB parameter limit),
+// set.p[m] being simulation m's, and zper is the z extent of one
+// simulation's grid, so block z = m zper + z'.  The body then reads its
+// arguments from the parameter space, which is read-only and which no
+// global store can alias, with a block-uniform index (no per-block copy, no
+// table in device memory).  A model on its own runs the same kernel with one
+// pack.
 template <class P>
-__global__ void __launch_bounds__(P::MAXT, P::MINB) ensemble_kernel(const P *__restrict__ tab, unsigned zper)
+struct PackSet {
+    static constexpr int FIT = (int)(30720 / sizeof(P));
+    static constexpr int N = FIT < 1 ? 1 : (FIT > 64 ? 64 : FIT);
+    P p[N];
+};
+
+template <class P>
+__global__ void __launch_bounds__(P::MAXT, P::MINB) ensemble_kernel(const __grid_constant__ PackSet<P> set, unsigned zper)
 {
-    static_assert(sizeof(P) % 8 == 0 && alignof(P) <= 8, "packs are copied in 8-byte words");
-    __shared__ __align__(16) unsigned long long sp[sizeof(P) / 8];
+    static_assert(sizeof(PackSet<P>) <= 32000, "kernel parameters are limited to 32 KB");
     const unsigned m = blockIdx.z / zper;
-    const unsigned long long *src = reinterpret_cast<const unsigned long long *>(tab + m);
-    for (unsigned i = threadIdx.x; i < sizeof(P) / 8; i += blockDim.x) sp[i] = src[i];
-    __syncthreads();
     const BlockIx b{blockIdx.x, blockIdx.y, blockIdx.z - m * zper, gridDim.x, gridDim.y, zper};
-    reinterpret_cast<const P *>(sp)->run(b);
+    set.p[m].run(b);
 }
 
 }  // namespace hydft

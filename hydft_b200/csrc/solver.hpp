@@ -60,8 +60,10 @@ struct LaunchRec {
     dim3 grid, block;
     size_t smem = 0;
     std::vector<unsigned char> pack;
-    // the ensemble form for n simulations whose packs are at tab (device)
-    void (*launch)(const void *tab, unsigned n, dim3 grid, dim3 block, size_t smem, cudaStream_t st) = nullptr;
+    unsigned per_launch = 1;          // simulations one launch of the ensemble form carries
+    // the ensemble form for n simulations whose packs lie back to back at
+    // `packs` (host memory; they travel as kernel parameters)
+    void (*launch)(const void *packs, unsigned n, dim3 grid, dim3 block, size_t smem, cudaStream_t st) = nullptr;
     // raises the ensemble form's dynamic shared-memory limit to smem
     cudaError_t (*prepare)(size_t smem) = nullptr;
 };

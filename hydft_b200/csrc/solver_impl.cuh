@@ -378,12 +378,21 @@ static bool has_plan(int L)
     return L == 32 || L == 48 || L == 64 || L == 96 || L == 128 || L == 256;
 }
 
-// The ensemble form of pack P's kernel for n simulations (LaunchRec::launch)
+// The ensemble form of pack P's kernel for n simulations whose packs lie
+// back to back at `packs` (host memory; LaunchRec::launch): one launch per
+// PackSet<P>::N simulations, each carrying its packs as its parameter
 template <class P>
-void ensemble_launch(const void *tab, unsigned n, dim3 grid, dim3 block, size_t smem, cudaStream_t st)
+void ensemble_launch(const void *packs, unsigned n, dim3 grid, dim3 block, size_t smem, cudaStream_t st)
 {
     static_assert(std::is_trivially_copyable<P>::value, "a pack is copied as bytes");
-    ensemble_kernel<P><<<dim3(grid.x, grid.y, grid.z * n), block, smem, st>>>(static_cast<const P *>(tab), grid.z);
+    const unsigned char *src = static_cast<const unsigned char *>(packs);
+    for (unsigned c = 0; c < n; c += PackSet<P>::N) {
+        const unsigned k = std::min<unsigned>(PackSet<P>::N, n - c);
+        PackSet<P> set;
+        std::memset(static_cast<void *>(&set), 0, sizeof(set));
+        std::memcpy(static_cast<void *>(set.p), src + (size_t)c * sizeof(P), (size_t)k * sizeof(P));
+        ensemble_kernel<P><<<dim3(grid.x, grid.y, grid.z * k), block, smem, st>>>(set, grid.z);
+    }
 }
 
 // Raises a kernel's dynamic shared-memory limit to all that the current
@@ -406,8 +415,8 @@ inline cudaError_t raise_smem_limit(const void *func, size_t need)
     return cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
 }
 
-// the dynamic shared-memory limit of the ensemble form; its static copy of
-// the pack counts against the default 48 KB, so the limit is always set
+// the dynamic shared-memory limit of the ensemble form, set for every
+// launch shape (the default limit is 48 KB)
 template <class P>
 cudaError_t ensemble_prepare(size_t smem)
 {
@@ -513,8 +522,6 @@ public:
     std::vector<LaunchRec> *rec = nullptr;
     bool rec_ok = true;
     // this solver's step packs (the ensemble-of-one form of its step)
-    void *packbuf = nullptr;
-    size_t packcap = 0;
 
     template <class F>
     void launch(const char *name, double bytes, F &&f)
@@ -562,6 +569,7 @@ public:
             r.smem = smem;
             r.pack.resize(sizeof(P));
             std::memcpy(r.pack.data(), &pack, sizeof(P));
+            r.per_launch = PackSet<P>::N;
             r.launch = &ensemble_launch<P>;
             r.prepare = &ensemble_prepare<P>;
             rec->push_back(std::move(r));
@@ -589,7 +597,6 @@ public:
         if (gexec) cudaGraphExecDestroy(gexec);
         if (graph) cudaGraphDestroy(graph);
         for (void *p : allocs) cudaFree(p);
-        if (packbuf) cudaFree(packbuf);
         if (st) cudaStreamDestroy(st);
     }
 
@@ -1126,9 +1133,8 @@ public:
                 int nt = std::min(256, x_ntmax) / T * T;
                 size_t sm = xstaged_smem<R, T, E>(nt, g.pkx, 4, 0);
                 // the blocks per SM the kernel is compiled for must fit: 228 KB
-                // of shared memory per SM, 1 KB reserved per block, and the
-                // ensemble form's copy of its pack
-                const size_t cap = (xstaged_minb<R, E>() == 2 ? 115712 : (size_t)smem_optin) - sizeof(pk);
+                // of shared memory per SM, 1 KB reserved per block
+                const size_t cap = xstaged_minb<R, E>() == 2 ? 115712 : (size_t)smem_optin;
                 while (sm > cap && nt > 32) {   // whole warps: each stages its own rows
                     nt /= 2;
                     sm = xstaged_smem<R, T, E>(nt, g.pkx, 4, 0);
@@ -1175,9 +1181,8 @@ public:
             auto go_rows = [&](auto k, auto pk, int nreal_rows) {
                 int nt = std::min(256, x_ntmax) / T * T;
                 size_t sm = xstaged_smem<R, T, E>(nt, g.pkx, 2, nreal_rows);
-                // two blocks per SM: 228 KB of shared memory, 1 KB reserved per
-                // block, and the ensemble form's copy of its pack
-                while (sm > 115712 - sizeof(pk) && nt > 32) {   // whole warps
+                // two blocks per SM: 228 KB of shared memory, 1 KB reserved per block
+                while (sm > 115712 && nt > 32) {   // whole warps
                     nt /= 2;
                     sm = xstaged_smem<R, T, E>(nt, g.pkx, 2, nreal_rows);
                 }
@@ -1500,7 +1505,7 @@ public:
             std::vector<LaunchRec> recs;
             std::vector<size_t> off;
             int rc = 0;
-            CK(cudaStreamSynchronize(st));   // the pack table is rewritten for every step
+            CK(cudaStreamSynchronize(st));
             const bool ens = upload_recorded(recs, off, rc);
             if (rc) { profiling = false; return rc; }
             if (ens) launch_recorded(recs, off);
@@ -1818,36 +1823,20 @@ public:
         return 0;
     }
 
-    // The step's launches as an ensemble of one: the packs of one recorded
-    // step in this solver's device table, each launch the ensemble form
-    // with n = 1, so that the model alone and the same model in an ensemble
-    // group run the same compiled kernels (bit-identical fields).
-    // upload_recorded records one step and uploads its packs (synchronously,
-    // outside any capture); it returns false, with nothing uploaded, when a
-    // launch of the step has no ensemble form.
+    // The step's launches as an ensemble of one: each launch of one recorded
+    // step is the ensemble form with n = 1 and the solver's own pack, so that
+    // the model alone and the same model in an ensemble group run the same
+    // compiled kernels (bit-identical fields).  upload_recorded records one
+    // step and prepares the ensemble forms (outside any capture); it returns
+    // false when a launch of the step has no ensemble form.
     bool upload_recorded(std::vector<LaunchRec> &recs, std::vector<size_t> &off, int &rc)
     {
         rc = 0;
         if (record_step(recs)) return false;
-        size_t total = 0;
         off.assign(recs.size(), 0);
-        for (size_t i = 0; i < recs.size(); ++i) {
-            off[i] = total;
-            total += (recs[i].pack.size() + 255) / 256 * 256;
-        }
-        if (total > packcap) {
-            if (packbuf) cudaFree(packbuf);
-            packbuf = nullptr;
-            packcap = 0;
-            cudaError_t e = cudaMalloc(&packbuf, total);
-            if (e != cudaSuccess) { err = std::string("cudaMalloc: ") + cudaGetErrorString(e); rc = HYDFT_E_OOM; return true; }
-            packcap = total;
-        }
-        std::vector<unsigned char> host(total, 0);
-        for (size_t i = 0; i < recs.size(); ++i) std::memcpy(host.data() + off[i], recs[i].pack.data(), recs[i].pack.size());
-        cudaError_t e = cudaMemcpy(packbuf, host.data(), total, cudaMemcpyHostToDevice);
+        cudaError_t e = cudaSuccess;
         for (size_t i = 0; e == cudaSuccess && i < recs.size(); ++i) e = recs[i].prepare(recs[i].smem);
-        if (e != cudaSuccess) { err = std::string("pack table: ") + cudaGetErrorString(e); rc = HYDFT_E_CUDA; }
+        if (e != cudaSuccess) { err = std::string("ensemble form: ") + cudaGetErrorString(e); rc = HYDFT_E_CUDA; }
         return true;
     }
 
@@ -1861,7 +1850,7 @@ public:
                 cudaEventCreate(&eb);
                 cudaEventRecord(ea, st);
             }
-            r.launch(static_cast<unsigned char *>(packbuf) + off[i], 1, r.grid, r.block, r.smem, st);
+            r.launch(r.pack.data(), 1, r.grid, r.block, r.smem, st);
             launches++;
             if (profiling) {
                 cudaEventRecord(eb, st);
@@ -1886,7 +1875,8 @@ public:
         if (nsteps <= 0) return 0;
         if (!gexec) {
             const int64_t before = launches;
-            // the packs are uploaded before the capture begins
+            // the step is recorded and its ensemble forms prepared before the
+            // capture begins
             std::vector<LaunchRec> recs;
             std::vector<size_t> off;
             int rc = 0;
