@@ -457,6 +457,73 @@ __global__ void __launch_bounds__(TX * T * G) zfwd_tma(const __grid_constant__ G
     zfwd_body<R, T, E, TX, G, BAND, NB>(bk, g, a, twz, norm, tile);
 }
 
+// The ensemble forms of the TMA passes: each pack carries its simulation's
+// tensor map (kernel parameter space, from which a tensor load may read its
+// map) and field coordinates, and runs the TMA kernel's body.
+template <typename R, int T, int E, int TX, int G, bool BAND>
+struct YinvTmaPack {
+    static constexpr int MAXT = TX * T * G, MINB = 1;
+    CUtensorMap tm;
+    Grid g;
+    PassArgs<R> a;
+    const cplx<R> *tw;
+    TmaFields tf;
+    __device__ __forceinline__ void run(const BlockIx &bk) const
+    {
+        bool ok;
+        const cplx<R> *tile = tma_tile_begin<R, T * E>(&tm, 2 * TX * (int)bk.x, 0, G * (int)bk.y, tf.src[bk.z],
+                                                       (unsigned)(2 * TX * g.nkyc * G * sizeof(R)), ok);
+        if (!ok) {
+            if (threadIdx.x == 0) atomicOr(tf.status, ST_TIMEOUT);
+            return;
+        }
+        yinv_body<R, T, E, TX, G, BAND>(bk, g, a, tw, tile);
+    }
+};
+
+template <typename R, int T, int E, int TX, int G, bool BAND>
+struct YfwdTmaPack {
+    static constexpr int MAXT = TX * T * G, MINB = 1;
+    CUtensorMap tm;
+    Grid g;
+    PassArgs<R> a;
+    const cplx<R> *tw;
+    TmaFields tf;
+    __device__ __forceinline__ void run(const BlockIx &bk) const
+    {
+        bool ok;
+        const cplx<R> *tile = tma_tile_begin<R, T * E>(&tm, 2 * TX * (int)bk.x, 0, G * (int)bk.y, tf.src[bk.z],
+                                                       (unsigned)(2 * TX * g.ny * G * sizeof(R)), ok);
+        if (!ok) {
+            if (threadIdx.x == 0) atomicOr(tf.status, ST_TIMEOUT);
+            return;
+        }
+        yfwd_body<R, T, E, TX, G, BAND>(bk, g, a, tw, tile);
+    }
+};
+
+template <typename R, int T, int E, int TX, int G, bool BAND, int NB>
+struct ZfwdTmaPack {
+    static constexpr int MAXT = TX * T * G, MINB = 1;
+    CUtensorMap tm;
+    Grid g;
+    PassArgs<R> a;
+    const cplx<R> *tw;
+    R norm;
+    TmaFields tf;
+    __device__ __forceinline__ void run(const BlockIx &bk) const
+    {
+        bool ok;
+        const cplx<R> *tile = tma_tile_begin<R, T * E>(&tm, 2 * TX * (int)bk.x, G * NB * (int)bk.y, 0, tf.src[bk.z],
+                                                       (unsigned)(2 * TX * G * NB * g.nz * sizeof(R)), ok);
+        if (!ok) {
+            if (threadIdx.x == 0) atomicOr(tf.status, ST_TIMEOUT);
+            return;
+        }
+        zfwd_body<R, T, E, TX, G, BAND, NB>(bk, g, a, tw, norm, tile);
+    }
+};
+
 // smem bytes of a y/z fast pass
 template <typename R>
 inline size_t yz_fast_smem(int L, int T, int TX, int G)

@@ -918,17 +918,21 @@ public:
                 set_smem(k, sm);
                 const dim3 grid((g.nkxc + TX - 1) / TX, (g.nkyc + G * nb - 1) / (G * nb), nzf);
                 pk.g = g; pk.a = a; pk.tw = tpz;
-                // TMA: one map per input field; the tile goes past the pass's
-                // own shared memory (it does not fit in the exchange buffer)
+                // TMA: one map per input field; the tile goes into the exchange
+                // buffer where it fits (every column is read into registers
+                // before the first exchange), else past the pass's own shared
+                // memory (with two rows per thread it does not fit)
                 const size_t tile = sizeof(cplx<R>) * (size_t)TX * G * nb * g.nkzc;
-                const size_t smt = (sm + tile + 8 + 127) / 128 * 128;
-                bool tma = !rec && use_tma && tma_zinv && nzf <= 16 && sm % 128 == 0 && smt <= (size_t)smem_optin;
+                const bool inbuf = tile + 8 <= sm - sizeof(cplx<R>) * 2 * T * E;
+                const size_t smt = inbuf ? sm : (sm + tile + 8 + 127) / 128 * 128;
+                bool tma = !rec && use_tma && tma_zinv && nzf <= 16 && (inbuf || sm % 128 == 0) &&
+                           smt <= (size_t)smem_optin;
                 TmaMaps maps;
                 for (int f = 0; tma && f < nzf; ++f)
                     tma = make_field_tmap<R>(&maps.m[f], a.in[f], g.pkx, g.nkyc, g.nkzc, 1, TX, G * nb, g.nkzc);
                 if (tma) {
                     set_smem(kt, smt);
-                    const unsigned off = (unsigned)(sm / sizeof(cplx<R>));
+                    const unsigned off = inbuf ? (unsigned)(2 * T * E) : (unsigned)(sm / sizeof(cplx<R>));
                     unsigned *stw = &ctrl->status;
                     launch("zinv", zbytes, [&] { kt<<<grid, TX * T * G, smt, st>>>(g, a, tpz, maps, off, stw); });
                     return;
@@ -966,22 +970,22 @@ public:
                 constexpr int G = yz_rows<T, TX, decltype(NTc)::value>();
                 const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
                 const dim3 grid((g.nkxc + TX - 1) / TX, (g.nz + G - 1) / G, nf);
-                auto go = [&](auto k, auto pk, auto kt) {
+                auto go = [&](auto k, auto pk, auto kt, auto pkt) {
                     set_smem(k, sm);
                     pk.g = g; pk.a = b; pk.tw = tpy;
                     const size_t tile = sizeof(cplx<R>) * (size_t)TX * g.nkyc * G;
-                    CUtensorMap tm;
-                    if (!rec && use_tma && tile + 8 <= sm - sizeof(cplx<R>) * 2 * T * E &&
-                        make_field_tmap<R>(&tm, zi, g.pkx, g.nkyc, g.nz, nin_max, TX, g.nkyc, G)) {
-                        const TmaFields tf = tma_fields(b.in, nf, zi, zsize);
+                    if (use_tma && tile + 8 <= sm - sizeof(cplx<R>) * 2 * T * E &&
+                        make_field_tmap<R>(&pkt.tm, zi, g.pkx, g.nkyc, g.nz, nin_max, TX, g.nkyc, G)) {
+                        pkt.g = g; pkt.a = b; pkt.tw = tpy; pkt.tf = tma_fields(b.in, nf, zi, zsize);
                         set_smem(kt, sm);
-                        launch("yinv", ybytes, [&] { kt<<<grid, TX * T * G, sm, st>>>(g, b, tpy, tm, tf); });
+                        launch_p("yinv", ybytes, grid, TX * T * G, sm, pkt,
+                                 [&] { kt<<<grid, TX * T * G, sm, st>>>(g, b, tpy, pkt.tm, pkt.tf); });
                         return;
                     }
                     launch_p("yinv", ybytes, grid, TX * T * G, sm, pk, [&] { k<<<grid, TX * T * G, sm, st>>>(g, b, tpy); });
                 };
-                if (band_y) go(yinv_fast<R, T, E, TX, G, true>, YinvPack<R, T, E, TX, G, true>{}, yinv_tma<R, T, E, TX, G, true>);
-                else go(yinv_fast<R, T, E, TX, G, false>, YinvPack<R, T, E, TX, G, false>{}, yinv_tma<R, T, E, TX, G, false>);
+                if (band_y) go(yinv_fast<R, T, E, TX, G, true>, YinvPack<R, T, E, TX, G, true>{}, yinv_tma<R, T, E, TX, G, true>, YinvTmaPack<R, T, E, TX, G, true>{});
+                else go(yinv_fast<R, T, E, TX, G, false>, YinvPack<R, T, E, TX, G, false>{}, yinv_tma<R, T, E, TX, G, false>, YinvTmaPack<R, T, E, TX, G, false>{});
             });
             });
             if (!yf) {
@@ -1013,22 +1017,22 @@ public:
                 constexpr int G = yz_rows<T, TX, decltype(NTc)::value>();
                 const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
                 const dim3 grid((g.nkxc + TX - 1) / TX, (g.nz + G - 1) / G, nf);
-                auto go = [&](auto k, auto pk, auto kt) {
+                auto go = [&](auto k, auto pk, auto kt, auto pkt) {
                     set_smem(k, sm);
                     pk.g = g; pk.a = b; pk.tw = tpy;
                     const size_t tile = sizeof(cplx<R>) * (size_t)TX * g.ny * G;
-                    CUtensorMap tm;
-                    if (!rec && use_tma && tile + 8 <= sm - sizeof(cplx<R>) * 2 * T * E &&
-                        make_field_tmap<R>(&tm, xo, g.pkx, g.ny, g.nz, nout_max, TX, g.ny, G)) {
-                        const TmaFields tf = tma_fields(b.in, nf, xo, ysize);
+                    if (use_tma && tile + 8 <= sm - sizeof(cplx<R>) * 2 * T * E &&
+                        make_field_tmap<R>(&pkt.tm, xo, g.pkx, g.ny, g.nz, nout_max, TX, g.ny, G)) {
+                        pkt.g = g; pkt.a = b; pkt.tw = tpy; pkt.tf = tma_fields(b.in, nf, xo, ysize);
                         set_smem(kt, sm);
-                        launch("yfwd", ybytes, [&] { kt<<<grid, TX * T * G, sm, st>>>(g, b, tpy, tm, tf); });
+                        launch_p("yfwd", ybytes, grid, TX * T * G, sm, pkt,
+                                 [&] { kt<<<grid, TX * T * G, sm, st>>>(g, b, tpy, pkt.tm, pkt.tf); });
                         return;
                     }
                     launch_p("yfwd", ybytes, grid, TX * T * G, sm, pk, [&] { k<<<grid, TX * T * G, sm, st>>>(g, b, tpy); });
                 };
-                if (band_y) go(yfwd_fast<R, T, E, TX, G, true>, YfwdPack<R, T, E, TX, G, true>{}, yfwd_tma<R, T, E, TX, G, true>);
-                else go(yfwd_fast<R, T, E, TX, G, false>, YfwdPack<R, T, E, TX, G, false>{}, yfwd_tma<R, T, E, TX, G, false>);
+                if (band_y) go(yfwd_fast<R, T, E, TX, G, true>, YfwdPack<R, T, E, TX, G, true>{}, yfwd_tma<R, T, E, TX, G, true>, YfwdTmaPack<R, T, E, TX, G, true>{});
+                else go(yfwd_fast<R, T, E, TX, G, false>, YfwdPack<R, T, E, TX, G, false>{}, yfwd_tma<R, T, E, TX, G, false>, YfwdTmaPack<R, T, E, TX, G, false>{});
             });
             });
             if (!yf) {
@@ -1052,27 +1056,27 @@ public:
             constexpr int TX = decltype(TXc)::value;
             constexpr int G = yz_rows<T, TX, decltype(NTc)::value>();
             const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
-            auto go = [&](auto k, auto pk, auto kt, int nb) {
+            auto go = [&](auto k, auto pk, auto kt, auto pkt, int nb) {
                 set_smem(k, sm);
                 const dim3 grid((g.nkxc + TX - 1) / TX, (g.nkyc + G * nb - 1) / (G * nb), nf);
                 pk.g = g; pk.a = a; pk.tw = tpz; pk.norm = norm;
                 const size_t tile = sizeof(cplx<R>) * (size_t)TX * G * nb * g.nz;
-                CUtensorMap tm;
-                if (!rec && use_tma && src == zi && tile + 8 <= sm - sizeof(cplx<R>) * 2 * T * E &&
-                    make_field_tmap<R>(&tm, zi, g.pkx, g.nkyc, g.nz, nin_max, TX, G * nb, g.nz)) {
-                    const TmaFields tf = tma_fields(a.in, nf, zi, zsize);
+                if (use_tma && src == zi && tile + 8 <= sm - sizeof(cplx<R>) * 2 * T * E &&
+                    make_field_tmap<R>(&pkt.tm, zi, g.pkx, g.nkyc, g.nz, nin_max, TX, G * nb, g.nz)) {
+                    pkt.g = g; pkt.a = a; pkt.tw = tpz; pkt.norm = norm; pkt.tf = tma_fields(a.in, nf, zi, zsize);
                     set_smem(kt, sm);
-                    launch("zfwd", zbytes, [&] { kt<<<grid, TX * T * G, sm, st>>>(g, a, tpz, norm, tm, tf); });
+                    launch_p("zfwd", zbytes, grid, TX * T * G, sm, pkt,
+                             [&] { kt<<<grid, TX * T * G, sm, st>>>(g, a, tpz, norm, pkt.tm, pkt.tf); });
                     return;
                 }
                 launch_p("zfwd", zbytes, grid, TX * T * G, sm, pk, [&] { k<<<grid, TX * T * G, sm, st>>>(g, a, tpz, norm); });
             };
             if (z_nbf == 2) {
-                if (band_z) go(zfwd_fast<R, T, E, TX, G, true, 2>, ZfwdPack<R, T, E, TX, G, true, 2>{}, zfwd_tma<R, T, E, TX, G, true, 2>, 2);
-                else go(zfwd_fast<R, T, E, TX, G, false, 2>, ZfwdPack<R, T, E, TX, G, false, 2>{}, zfwd_tma<R, T, E, TX, G, false, 2>, 2);
+                if (band_z) go(zfwd_fast<R, T, E, TX, G, true, 2>, ZfwdPack<R, T, E, TX, G, true, 2>{}, zfwd_tma<R, T, E, TX, G, true, 2>, ZfwdTmaPack<R, T, E, TX, G, true, 2>{}, 2);
+                else go(zfwd_fast<R, T, E, TX, G, false, 2>, ZfwdPack<R, T, E, TX, G, false, 2>{}, zfwd_tma<R, T, E, TX, G, false, 2>, ZfwdTmaPack<R, T, E, TX, G, false, 2>{}, 2);
             } else {
-                if (band_z) go(zfwd_fast<R, T, E, TX, G, true, 1>, ZfwdPack<R, T, E, TX, G, true, 1>{}, zfwd_tma<R, T, E, TX, G, true, 1>, 1);
-                else go(zfwd_fast<R, T, E, TX, G, false, 1>, ZfwdPack<R, T, E, TX, G, false, 1>{}, zfwd_tma<R, T, E, TX, G, false, 1>, 1);
+                if (band_z) go(zfwd_fast<R, T, E, TX, G, true, 1>, ZfwdPack<R, T, E, TX, G, true, 1>{}, zfwd_tma<R, T, E, TX, G, true, 1>, ZfwdTmaPack<R, T, E, TX, G, true, 1>{}, 1);
+                else go(zfwd_fast<R, T, E, TX, G, false, 1>, ZfwdPack<R, T, E, TX, G, false, 1>{}, zfwd_tma<R, T, E, TX, G, false, 1>, ZfwdTmaPack<R, T, E, TX, G, false, 1>{}, 1);
             }
             });
         });
