@@ -135,7 +135,8 @@ __device__ __forceinline__ void store_block(cplx<R> *__restrict__ col, const cpl
 // first is transformed, so that a thread keeps NB x E loads in flight
 template <typename R, int T, int E, int TX, int G, bool BAND, int NB>
 __device__ __forceinline__ void zinv_body(const BlockIx &bk, const Grid &g, const PassArgs<R> &a, const cplx<R> *twz,
-                                          const cplx<R> *tile = nullptr)
+                                          const cplx<R> *tile = nullptr, const CUtensorMap *otm = nullptr,
+                                          int odst = 0)
 {
     constexpr int L = T * E;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -197,6 +198,13 @@ __device__ __forceinline__ void zinv_body(const BlockIx &bk, const Grid &g, cons
         }
         if (b == 0) __syncthreads();   // the twiddles (later rows: the exchange's own barriers)
         stride_to_block<T, E, +1, R, BarBlock, TX>(v[b], t, xb + gi * (L + L / T) * TX + c, tw);
+        if (NB == 1 && otm) {
+            // output tile [nz][G][TX] in the exchange space (nz = L <= the
+            // space's L + L/T rows per G row), one tensor store
+            store_block<R, T, E>(xb + (size_t)gi * TX + c, v[b], G * TX, t);
+            tma_store_tile_4d(otm, xb, 2 * TX * (int)bk.x, G * (int)bk.y, 0, odst);
+            return;
+        }
         // z runs over the full axis: element stride nkyc * pkx in the ZI layout
         if (valid) store_block<R, T, E>(a.out[f] + (size_t)kyc * g.pkx + x, v[b], rs, t);
     }
@@ -219,7 +227,8 @@ struct ZinvPack {
 
 template <typename R, int T, int E, int TX, int G, bool BAND>
 __device__ __forceinline__ void yinv_body(const BlockIx &bk, const Grid &g, const PassArgs<R> &a, const cplx<R> *twy,
-                                          const cplx<R> *tile = nullptr)
+                                          const cplx<R> *tile = nullptr, const CUtensorMap *otm = nullptr,
+                                          int odst = 0)
 {
     constexpr int L = T * E;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -244,6 +253,17 @@ __device__ __forceinline__ void yinv_body(const BlockIx &bk, const Grid &g, cons
     }
     __syncthreads();
     stride_to_block<T, E, +1, R, BarBlock, TX>(v, t, xb + gi * (L + L / T) * TX + c, tw);
+    if (otm) {
+        // the exchange ended with a block barrier, so its space holds the
+        // output tile [G][ny][TX] (ny <= L + L/T); columns past the band
+        // hold zeros and land in the row padding, z planes past the grid
+        // are clipped by the tensor store
+        cplx<R> *ot = xb + (size_t)gi * g.ny * TX + c;
+#pragma unroll
+        for (int r = 0; r < E; ++r) ot[(size_t)block_pos<T, E>(t, r) * TX] = v[r];
+        tma_store_tile_4d(otm, xb, 2 * TX * (int)bk.x, 0, G * (int)bk.y, odst);
+        return;
+    }
     if (valid) store_block<R, T, E>(a.out[f] + (size_t)z * g.ny * g.pkx + x, v, g.pkx, t);
 }
 
@@ -264,7 +284,8 @@ struct YinvPack {
 
 template <typename R, int T, int E, int TX, int G, bool BAND>
 __device__ __forceinline__ void yfwd_body(const BlockIx &bk, const Grid &g, const PassArgs<R> &a, const cplx<R> *twy,
-                                          const cplx<R> *tile = nullptr)
+                                          const cplx<R> *tile = nullptr, const CUtensorMap *otm = nullptr,
+                                          int odst = 0)
 {
     constexpr int L = T * E;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -281,6 +302,13 @@ __device__ __forceinline__ void yfwd_body(const BlockIx &bk, const Grid &g, cons
         load_block<R, T, E>(v, a.in[f] + (size_t)z * g.ny * g.pkx + x, g.pkx, t, valid);
     __syncthreads();
     block_to_stride<T, E, -1, R, BarBlock, TX>(v, t, xb + gi * (L + L / T) * TX + c, tw);
+    if (otm) {
+        // output tile [G][nkyc][TX] in the exchange space (free after the
+        // exchange's closing barrier); see yinv_body
+        store_band<R, T, E, BAND>(xb + (size_t)gi * g.nkyc * TX + c, v, TX, t, g.My, g.nkyc, R(1));
+        tma_store_tile_4d(otm, xb, 2 * TX * (int)bk.x, 0, G * (int)bk.y, odst);
+        return;
+    }
     if (valid) store_band<R, T, E, BAND>(a.out[f] + (size_t)z * g.nkyc * g.pkx + x, v, g.pkx, t, g.My, g.nkyc, R(1));
 }
 
@@ -301,7 +329,7 @@ struct YfwdPack {
 
 template <typename R, int T, int E, int TX, int G, bool BAND, int NB>
 __device__ __forceinline__ void zfwd_body(const BlockIx &bk, const Grid &g, const PassArgs<R> &a, const cplx<R> *twz, R norm,
-                                          const cplx<R> *tile = nullptr)
+                                          const cplx<R> *tile = nullptr, const CUtensorMap *otm = nullptr)
 {
     constexpr int L = T * E;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -327,6 +355,13 @@ __device__ __forceinline__ void zfwd_body(const BlockIx &bk, const Grid &g, cons
         const bool valid = x < g.nkxc && kyc < g.nkyc;
         if (b == 0) __syncthreads();   // the twiddles (later rows: the exchange's own barriers)
         block_to_stride<T, E, -1, R, BarBlock, TX>(v[b], t, xb + gi * (L + L / T) * TX + c, tw);
+        if (NB == 1 && otm) {
+            // output tile [nkzc][G][TX] of field f's compact array (map otm
+            // covers that field alone), in the exchange space
+            store_band<R, T, E, BAND>(xb + (size_t)gi * TX + c, v[b], G * TX, t, g.Mz, g.nkzc, norm);
+            tma_store_tile_4d(otm, xb, 2 * TX * (int)bk.x, G * (int)bk.y, 0, 0);
+            return;
+        }
         if (valid) store_band<R, T, E, BAND>(a.out[f] + (size_t)kyc * g.pkx + x, v[b], rs, t, g.Mz, g.nkzc, norm);
     }
 }
@@ -355,6 +390,7 @@ struct ZfwdPack {
 // ST_TIMEOUT in *status and the block returns without storing.
 struct TmaFields {
     int src[MAXF];
+    int dst[MAXF];     // output field coordinate (passes with a tensor store)
     unsigned *status;
 };
 
@@ -425,6 +461,24 @@ __global__ void __launch_bounds__(TX * T * G) yinv_tma(const __grid_constant__ G
     yinv_body<R, T, E, TX, G, BAND>(bk, g, a, twy, tile);
 }
 
+// The y inverse pass with a tensor load of its input tile and a tensor
+// store of its output tile (map otm over the YI buffer)
+template <typename R, int T, int E, int TX, int G, bool BAND>
+__global__ void __launch_bounds__(TX * T * G) yinv_tma_st(const __grid_constant__ Grid g,
+    const __grid_constant__ PassArgs<R> a, const cplx<R> *twy, const __grid_constant__ CUtensorMap tm,
+    const __grid_constant__ CUtensorMap otm, const __grid_constant__ TmaFields tf)
+{
+    const BlockIx bk = hw_block();
+    bool ok;
+    const cplx<R> *tile = tma_tile_begin<R, T * E>(&tm, 2 * TX * (int)bk.x, 0, G * (int)bk.y, tf.src[bk.z],
+                                                   (unsigned)(2 * TX * g.nkyc * G * sizeof(R)), ok);
+    if (!ok) {
+        if (threadIdx.x == 0) atomicOr(tf.status, ST_TIMEOUT);
+        return;
+    }
+    yinv_body<R, T, E, TX, G, BAND>(bk, g, a, twy, tile, &otm, tf.dst[bk.z]);
+}
+
 template <typename R, int T, int E, int TX, int G, bool BAND>
 __global__ void __launch_bounds__(TX * T * G) yfwd_tma(const __grid_constant__ Grid g, const __grid_constant__ PassArgs<R> a,
                                                       const cplx<R> *twy, const __grid_constant__ CUtensorMap tm,
@@ -455,6 +509,53 @@ __global__ void __launch_bounds__(TX * T * G) zfwd_tma(const __grid_constant__ G
         return;
     }
     zfwd_body<R, T, E, TX, G, BAND, NB>(bk, g, a, twz, norm, tile);
+}
+
+// The forward y pass with tensor load and tensor store (map otm over the
+// ZI buffer)
+template <typename R, int T, int E, int TX, int G, bool BAND>
+__global__ void __launch_bounds__(TX * T * G) yfwd_tma_st(const __grid_constant__ Grid g,
+    const __grid_constant__ PassArgs<R> a, const cplx<R> *twy, const __grid_constant__ CUtensorMap tm,
+    const __grid_constant__ CUtensorMap otm, const __grid_constant__ TmaFields tf)
+{
+    const BlockIx bk = hw_block();
+    bool ok;
+    const cplx<R> *tile = tma_tile_begin<R, T * E>(&tm, 2 * TX * (int)bk.x, 0, G * (int)bk.y, tf.src[bk.z],
+                                                   (unsigned)(2 * TX * g.ny * G * sizeof(R)), ok);
+    if (!ok) {
+        if (threadIdx.x == 0) atomicOr(tf.status, ST_TIMEOUT);
+        return;
+    }
+    yfwd_body<R, T, E, TX, G, BAND>(bk, g, a, twy, tile, &otm, tf.dst[bk.z]);
+}
+
+// The forward z pass (one row per thread) with tensor load and a tensor
+// store into each output field's compact array (om.m[f] covers field f)
+template <typename R, int T, int E, int TX, int G, bool BAND>
+__global__ void __launch_bounds__(TX * T * G) zfwd_tma_st(const __grid_constant__ Grid g,
+    const __grid_constant__ PassArgs<R> a, const cplx<R> *twz, R norm, const __grid_constant__ CUtensorMap tm,
+    const __grid_constant__ TmaMaps om, const __grid_constant__ TmaFields tf)
+{
+    const BlockIx bk = hw_block();
+    bool ok;
+    const cplx<R> *tile = tma_tile_begin<R, T * E>(&tm, 2 * TX * (int)bk.x, G * (int)bk.y, 0, tf.src[bk.z],
+                                                   (unsigned)(2 * TX * G * g.nz * sizeof(R)), ok);
+    if (!ok) {
+        if (threadIdx.x == 0) atomicOr(tf.status, ST_TIMEOUT);
+        return;
+    }
+    zfwd_body<R, T, E, TX, G, BAND, 1>(bk, g, a, twz, norm, tile, &om.m[bk.z]);
+}
+
+// The inverse z pass (one row per thread) with a tensor store of its output
+// tile (map otm over the ZI buffer, field coordinate dst[f])
+template <typename R, int T, int E, int TX, int G, bool BAND>
+__global__ void __launch_bounds__(TX * T * G) zinv_st(const __grid_constant__ Grid g,
+    const __grid_constant__ PassArgs<R> a, const cplx<R> *twz, const __grid_constant__ CUtensorMap otm,
+    const __grid_constant__ TmaFields tf)
+{
+    const BlockIx bk = hw_block();
+    zinv_body<R, T, E, TX, G, BAND, 1>(bk, g, a, twz, nullptr, &otm, tf.dst[bk.z]);
 }
 
 // The ensemble forms of the TMA passes: each pack carries its simulation's

@@ -471,10 +471,12 @@ public:
     // register-FFT passes classify band elements at compile time
     // (HYDFT_BAND=0 selects the runtime test everywhere)
     bool band_x = false, band_y = false, band_z = false;
-    // ky rows per thread in the inverse z pass (HYDFT_ZNB=1 for one) and the
-    // forward one (HYDFT_ZNB_FWD=2 for two): at 256^3 two rows made the
-    // inverse 10 % faster and the forward 4 % slower (same-box A/B)
-    int z_nb = 2, z_nbf = 1;
+    // ky rows per thread in the inverse z pass (HYDFT_ZNB) and the forward
+    // one (HYDFT_ZNB_FWD=2 for two; at 256^3 two rows made the forward 4 %
+    // slower, same-box A/B).  Inverse: one on the plain path (its
+    // output tile then goes out by one tensor store), two in the ensemble
+    // forms (all loads in flight at once); HYDFT_ZNB = 1 | 2 sets both
+    int z_nb = 1, z_nb_ens = 2, z_nbf = 1;
     // the y inverse, y forward and z forward passes of the plain path read
     // each block's input tile with one TMA tensor load (HYDFT_TMA=0: every
     // thread loads its own elements, as the ensemble forms always do; the
@@ -484,13 +486,20 @@ public:
     // in the exchange buffer, and the extra shared memory costs blocks per SM
     // (256^3 step 6.17 against 6.06 ms without it), so it is off by default
     bool tma_zinv = false;
+    // tensor stores of the output tiles on the plain path: y inverse, y
+    // forward, z forward, z inverse with one row per thread
+    // (HYDFT_TMA_YST / _YFST / _ZFST / _ZIST = 0 switch them off)
+    bool tma_yst = true, tma_yfst = true, tma_zfst = true, tma_zist = true;
 
     // field coordinates of the pass inputs in[0..nf-1] within the buffer
     // base (fields `stride` complex values apart), for a TMA tensor map
     TmaFields tma_fields(const cplx<R> *const *in, int nf, const cplx<R> *base, size_t stride)
     {
         TmaFields tf;
-        for (int f = 0; f < MAXF; ++f) tf.src[f] = f < nf ? (int)((in[f] - base) / (ptrdiff_t)stride) : 0;
+        for (int f = 0; f < MAXF; ++f) {
+            tf.src[f] = f < nf ? (int)((in[f] - base) / (ptrdiff_t)stride) : 0;
+            tf.dst[f] = 0;
+        }
         tf.status = &ctrl->status;
         return tf;
     }
@@ -779,13 +788,21 @@ public:
             const char *ev = std::getenv("HYDFT_XPASS");
             if (ev && std::string(ev) == "v1") staged_x = false;
             const char *zn = std::getenv("HYDFT_ZNB");
-            if (zn && std::string(zn) == "1") z_nb = 1;
+            if (zn && (std::string(zn) == "1" || std::string(zn) == "2")) z_nb = z_nb_ens = std::atoi(zn);
             const char *znf = std::getenv("HYDFT_ZNB_FWD");
             if (znf && std::string(znf) == "2") z_nbf = 2;
             const char *et = std::getenv("HYDFT_TMA");
             if (et && std::string(et) == "0") use_tma = false;
             const char *ez = std::getenv("HYDFT_TMA_ZINV");
             if (ez) tma_zinv = std::string(ez) == "1";
+            auto flag = [](const char *name, bool &v) {
+                const char *e = std::getenv(name);
+                if (e && *e) v = std::string(e) == "1";
+            };
+            flag("HYDFT_TMA_YST", tma_yst);
+            flag("HYDFT_TMA_YFST", tma_yfst);
+            flag("HYDFT_TMA_ZFST", tma_zfst);
+            flag("HYDFT_TMA_ZIST", tma_zist);
             const char *eb = std::getenv("HYDFT_BAND");
             const bool band_ok = !(eb && std::string(eb) == "0");
             band_x = band_ok && g.Mx == (g.nx - 1) / 3;
@@ -914,10 +931,21 @@ public:
             constexpr int TX = decltype(TXc)::value;
             constexpr int G = yz_rows<T, TX, decltype(NTc)::value>();
             const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
-            auto go = [&](auto k, auto pk, auto kt, int nb) {
+            auto go = [&](auto k, auto pk, auto kt, auto kst, int nb) {
                 set_smem(k, sm);
                 const dim3 grid((g.nkxc + TX - 1) / TX, (g.nkyc + G * nb - 1) / (G * nb), nzf);
                 pk.g = g; pk.a = a; pk.tw = tpz;
+                // one row per thread: the output tile by a tensor store (the
+                // tile [nz][G][TX] fits in the exchange space)
+                CUtensorMap otm;
+                if (!rec && use_tma && tma_zist && nb == 1 && (size_t)g.nz * G * TX <= (size_t)G * (T * E + E) * TX &&
+                    make_field_tmap<R>(&otm, zi, g.pkx, g.nkyc, g.nz, nin_max, TX, G, g.nz)) {
+                    TmaFields tf = tma_fields(a.in, 0, zi, zsize);
+                    for (int f = 0; f < nzf; ++f) tf.dst[f] = (int)((a.out[f] - zi) / (ptrdiff_t)zsize);
+                    set_smem(kst, sm);
+                    launch("zinv", zbytes, [&] { kst<<<grid, TX * T * G, sm, st>>>(g, a, tpz, otm, tf); });
+                    return;
+                }
                 // TMA: one map per input field; the tile goes into the exchange
                 // buffer where it fits (every column is read into registers
                 // before the first exchange), else past the pass's own shared
@@ -939,12 +967,12 @@ public:
                 }
                 launch_p("zinv", zbytes, grid, TX * T * G, sm, pk, [&] { k<<<grid, TX * T * G, sm, st>>>(g, a, tpz); });
             };
-            if (z_nb == 2) {
-                if (band_z) go(zinv_fast<R, T, E, TX, G, true, 2>, ZinvPack<R, T, E, TX, G, true, 2>{}, zinv_tma<R, T, E, TX, G, true, 2>, 2);
-                else go(zinv_fast<R, T, E, TX, G, false, 2>, ZinvPack<R, T, E, TX, G, false, 2>{}, zinv_tma<R, T, E, TX, G, false, 2>, 2);
+            if ((rec ? z_nb_ens : z_nb) == 2) {
+                if (band_z) go(zinv_fast<R, T, E, TX, G, true, 2>, ZinvPack<R, T, E, TX, G, true, 2>{}, zinv_tma<R, T, E, TX, G, true, 2>, zinv_st<R, T, E, TX, G, true>, 2);
+                else go(zinv_fast<R, T, E, TX, G, false, 2>, ZinvPack<R, T, E, TX, G, false, 2>{}, zinv_tma<R, T, E, TX, G, false, 2>, zinv_st<R, T, E, TX, G, false>, 2);
             } else {
-                if (band_z) go(zinv_fast<R, T, E, TX, G, true, 1>, ZinvPack<R, T, E, TX, G, true, 1>{}, zinv_tma<R, T, E, TX, G, true, 1>, 1);
-                else go(zinv_fast<R, T, E, TX, G, false, 1>, ZinvPack<R, T, E, TX, G, false, 1>{}, zinv_tma<R, T, E, TX, G, false, 1>, 1);
+                if (band_z) go(zinv_fast<R, T, E, TX, G, true, 1>, ZinvPack<R, T, E, TX, G, true, 1>{}, zinv_tma<R, T, E, TX, G, true, 1>, zinv_st<R, T, E, TX, G, true>, 1);
+                else go(zinv_fast<R, T, E, TX, G, false, 1>, ZinvPack<R, T, E, TX, G, false, 1>{}, zinv_tma<R, T, E, TX, G, false, 1>, zinv_st<R, T, E, TX, G, false>, 1);
             }
             });
         });
@@ -970,13 +998,21 @@ public:
                 constexpr int G = yz_rows<T, TX, decltype(NTc)::value>();
                 const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
                 const dim3 grid((g.nkxc + TX - 1) / TX, (g.nz + G - 1) / G, nf);
-                auto go = [&](auto k, auto pk, auto kt, auto pkt) {
+                auto go = [&](auto k, auto pk, auto kt, auto pkt, auto kst) {
                     set_smem(k, sm);
                     pk.g = g; pk.a = b; pk.tw = tpy;
                     const size_t tile = sizeof(cplx<R>) * (size_t)TX * g.nkyc * G;
                     if (use_tma && tile + 8 <= sm - sizeof(cplx<R>) * 2 * T * E &&
                         make_field_tmap<R>(&pkt.tm, zi, g.pkx, g.nkyc, g.nz, nin_max, TX, g.nkyc, G)) {
                         pkt.g = g; pkt.a = b; pkt.tw = tpy; pkt.tf = tma_fields(b.in, nf, zi, zsize);
+                        // the output tile by a tensor store as well (HYDFT_TMA_YST=1)
+                        CUtensorMap otm;
+                        if (!rec && tma_yst && make_field_tmap<R>(&otm, yi, g.pkx, g.ny, g.nz, nin_max, TX, g.ny, G)) {
+                            for (int f = 0; f < nf; ++f) pkt.tf.dst[f] = (int)((b.out[f] - yi) / (ptrdiff_t)ysize);
+                            set_smem(kst, sm);
+                            launch("yinv", ybytes, [&] { kst<<<grid, TX * T * G, sm, st>>>(g, b, tpy, pkt.tm, otm, pkt.tf); });
+                            return;
+                        }
                         set_smem(kt, sm);
                         launch_p("yinv", ybytes, grid, TX * T * G, sm, pkt,
                                  [&] { kt<<<grid, TX * T * G, sm, st>>>(g, b, tpy, pkt.tm, pkt.tf); });
@@ -984,8 +1020,8 @@ public:
                     }
                     launch_p("yinv", ybytes, grid, TX * T * G, sm, pk, [&] { k<<<grid, TX * T * G, sm, st>>>(g, b, tpy); });
                 };
-                if (band_y) go(yinv_fast<R, T, E, TX, G, true>, YinvPack<R, T, E, TX, G, true>{}, yinv_tma<R, T, E, TX, G, true>, YinvTmaPack<R, T, E, TX, G, true>{});
-                else go(yinv_fast<R, T, E, TX, G, false>, YinvPack<R, T, E, TX, G, false>{}, yinv_tma<R, T, E, TX, G, false>, YinvTmaPack<R, T, E, TX, G, false>{});
+                if (band_y) go(yinv_fast<R, T, E, TX, G, true>, YinvPack<R, T, E, TX, G, true>{}, yinv_tma<R, T, E, TX, G, true>, YinvTmaPack<R, T, E, TX, G, true>{}, yinv_tma_st<R, T, E, TX, G, true>);
+                else go(yinv_fast<R, T, E, TX, G, false>, YinvPack<R, T, E, TX, G, false>{}, yinv_tma<R, T, E, TX, G, false>, YinvTmaPack<R, T, E, TX, G, false>{}, yinv_tma_st<R, T, E, TX, G, false>);
             });
             });
             if (!yf) {
@@ -1017,13 +1053,21 @@ public:
                 constexpr int G = yz_rows<T, TX, decltype(NTc)::value>();
                 const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
                 const dim3 grid((g.nkxc + TX - 1) / TX, (g.nz + G - 1) / G, nf);
-                auto go = [&](auto k, auto pk, auto kt, auto pkt) {
+                auto go = [&](auto k, auto pk, auto kt, auto pkt, auto kst) {
                     set_smem(k, sm);
                     pk.g = g; pk.a = b; pk.tw = tpy;
                     const size_t tile = sizeof(cplx<R>) * (size_t)TX * g.ny * G;
                     if (use_tma && tile + 8 <= sm - sizeof(cplx<R>) * 2 * T * E &&
                         make_field_tmap<R>(&pkt.tm, xo, g.pkx, g.ny, g.nz, nout_max, TX, g.ny, G)) {
                         pkt.g = g; pkt.a = b; pkt.tw = tpy; pkt.tf = tma_fields(b.in, nf, xo, ysize);
+                        // the output tile [G][nkyc][TX] by a tensor store as well
+                        CUtensorMap otm;
+                        if (!rec && tma_yfst && make_field_tmap<R>(&otm, zi, g.pkx, g.nkyc, g.nz, nin_max, TX, g.nkyc, G)) {
+                            for (int f = 0; f < nf; ++f) pkt.tf.dst[f] = (int)((b.out[f] - zi) / (ptrdiff_t)zsize);
+                            set_smem(kst, sm);
+                            launch("yfwd", ybytes, [&] { kst<<<grid, TX * T * G, sm, st>>>(g, b, tpy, pkt.tm, otm, pkt.tf); });
+                            return;
+                        }
                         set_smem(kt, sm);
                         launch_p("yfwd", ybytes, grid, TX * T * G, sm, pkt,
                                  [&] { kt<<<grid, TX * T * G, sm, st>>>(g, b, tpy, pkt.tm, pkt.tf); });
@@ -1031,8 +1075,8 @@ public:
                     }
                     launch_p("yfwd", ybytes, grid, TX * T * G, sm, pk, [&] { k<<<grid, TX * T * G, sm, st>>>(g, b, tpy); });
                 };
-                if (band_y) go(yfwd_fast<R, T, E, TX, G, true>, YfwdPack<R, T, E, TX, G, true>{}, yfwd_tma<R, T, E, TX, G, true>, YfwdTmaPack<R, T, E, TX, G, true>{});
-                else go(yfwd_fast<R, T, E, TX, G, false>, YfwdPack<R, T, E, TX, G, false>{}, yfwd_tma<R, T, E, TX, G, false>, YfwdTmaPack<R, T, E, TX, G, false>{});
+                if (band_y) go(yfwd_fast<R, T, E, TX, G, true>, YfwdPack<R, T, E, TX, G, true>{}, yfwd_tma<R, T, E, TX, G, true>, YfwdTmaPack<R, T, E, TX, G, true>{}, yfwd_tma_st<R, T, E, TX, G, true>);
+                else go(yfwd_fast<R, T, E, TX, G, false>, YfwdPack<R, T, E, TX, G, false>{}, yfwd_tma<R, T, E, TX, G, false>, YfwdTmaPack<R, T, E, TX, G, false>{}, yfwd_tma_st<R, T, E, TX, G, false>);
             });
             });
             if (!yf) {
@@ -1056,7 +1100,7 @@ public:
             constexpr int TX = decltype(TXc)::value;
             constexpr int G = yz_rows<T, TX, decltype(NTc)::value>();
             const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
-            auto go = [&](auto k, auto pk, auto kt, auto pkt, int nb) {
+            auto go = [&](auto k, auto pk, auto kt, auto pkt, auto kst, int nb) {
                 set_smem(k, sm);
                 const dim3 grid((g.nkxc + TX - 1) / TX, (g.nkyc + G * nb - 1) / (G * nb), nf);
                 pk.g = g; pk.a = a; pk.tw = tpz; pk.norm = norm;
@@ -1064,6 +1108,17 @@ public:
                 if (use_tma && src == zi && tile + 8 <= sm - sizeof(cplx<R>) * 2 * T * E &&
                     make_field_tmap<R>(&pkt.tm, zi, g.pkx, g.nkyc, g.nz, nin_max, TX, G * nb, g.nz)) {
                     pkt.g = g; pkt.a = a; pkt.tw = tpz; pkt.norm = norm; pkt.tf = tma_fields(a.in, nf, zi, zsize);
+                    // one row per thread: each output field's tile [nkzc][G][TX]
+                    // by a tensor store (one map per compact output field)
+                    bool stv = !rec && tma_zfst && nb == 1 && nf <= 16;
+                    TmaMaps om;
+                    for (int f = 0; stv && f < nf; ++f)
+                        stv = make_field_tmap<R>(&om.m[f], a.out[f], g.pkx, g.nkyc, g.nkzc, 1, TX, G, g.nkzc);
+                    if (stv) {
+                        set_smem(kst, sm);
+                        launch("zfwd", zbytes, [&] { kst<<<grid, TX * T * G, sm, st>>>(g, a, tpz, norm, pkt.tm, om, pkt.tf); });
+                        return;
+                    }
                     set_smem(kt, sm);
                     launch_p("zfwd", zbytes, grid, TX * T * G, sm, pkt,
                              [&] { kt<<<grid, TX * T * G, sm, st>>>(g, a, tpz, norm, pkt.tm, pkt.tf); });
@@ -1072,11 +1127,11 @@ public:
                 launch_p("zfwd", zbytes, grid, TX * T * G, sm, pk, [&] { k<<<grid, TX * T * G, sm, st>>>(g, a, tpz, norm); });
             };
             if (z_nbf == 2) {
-                if (band_z) go(zfwd_fast<R, T, E, TX, G, true, 2>, ZfwdPack<R, T, E, TX, G, true, 2>{}, zfwd_tma<R, T, E, TX, G, true, 2>, ZfwdTmaPack<R, T, E, TX, G, true, 2>{}, 2);
-                else go(zfwd_fast<R, T, E, TX, G, false, 2>, ZfwdPack<R, T, E, TX, G, false, 2>{}, zfwd_tma<R, T, E, TX, G, false, 2>, ZfwdTmaPack<R, T, E, TX, G, false, 2>{}, 2);
+                if (band_z) go(zfwd_fast<R, T, E, TX, G, true, 2>, ZfwdPack<R, T, E, TX, G, true, 2>{}, zfwd_tma<R, T, E, TX, G, true, 2>, ZfwdTmaPack<R, T, E, TX, G, true, 2>{}, zfwd_tma_st<R, T, E, TX, G, true>, 2);
+                else go(zfwd_fast<R, T, E, TX, G, false, 2>, ZfwdPack<R, T, E, TX, G, false, 2>{}, zfwd_tma<R, T, E, TX, G, false, 2>, ZfwdTmaPack<R, T, E, TX, G, false, 2>{}, zfwd_tma_st<R, T, E, TX, G, false>, 2);
             } else {
-                if (band_z) go(zfwd_fast<R, T, E, TX, G, true, 1>, ZfwdPack<R, T, E, TX, G, true, 1>{}, zfwd_tma<R, T, E, TX, G, true, 1>, ZfwdTmaPack<R, T, E, TX, G, true, 1>{}, 1);
-                else go(zfwd_fast<R, T, E, TX, G, false, 1>, ZfwdPack<R, T, E, TX, G, false, 1>{}, zfwd_tma<R, T, E, TX, G, false, 1>, ZfwdTmaPack<R, T, E, TX, G, false, 1>{}, 1);
+                if (band_z) go(zfwd_fast<R, T, E, TX, G, true, 1>, ZfwdPack<R, T, E, TX, G, true, 1>{}, zfwd_tma<R, T, E, TX, G, true, 1>, ZfwdTmaPack<R, T, E, TX, G, true, 1>{}, zfwd_tma_st<R, T, E, TX, G, true>, 1);
+                else go(zfwd_fast<R, T, E, TX, G, false, 1>, ZfwdPack<R, T, E, TX, G, false, 1>{}, zfwd_tma<R, T, E, TX, G, false, 1>, ZfwdTmaPack<R, T, E, TX, G, false, 1>{}, zfwd_tma_st<R, T, E, TX, G, false>, 1);
             }
             });
         });

@@ -121,6 +121,26 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *tm, in
         : "memory");
 }
 
+// The block's tile at src (shared memory, 128-byte aligned) written to the
+// tensor of map *tm at scalar coordinates (c0, c1, c2, c3), none negative
+// and c0 a multiple of 16 bytes; elements past the tensor's edges are
+// clipped.  Every thread's writes of the tile come first (proxy fence and
+// barrier); thread 0 issues the store and waits until it has read the tile,
+// so the block's shared memory outlives the read.  No multicast.
+__device__ __forceinline__ void tma_store_tile_4d(const CUtensorMap *tm, const void *src, int c0, int c1, int c2, int c3)
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4}], [%5];" ::"l"(
+                         reinterpret_cast<uint64_t>(tm)),
+                     "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(src))
+                     : "memory");
+        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+    }
+}
+
 // One untiled bulk copy of `bytes` (a multiple of 16) from global memory
 // into this CTA's shared memory, completing on bar; both addresses 16-byte
 // aligned; no multicast, and the source is this GPU's memory.

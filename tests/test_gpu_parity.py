@@ -370,14 +370,22 @@ def test_tma_tile_loads_give_identical_results(hg, monkeypatch, prec):
     """The y inverse, y forward and z forward passes of a 128^3 model (which
     steps with the plain kernels) read their input tiles with TMA tensor
     loads, and with HYDFT_TMA_ZINV=1 the z inverse pass too; with
+    HYDFT_TMA_YST / _YFST / _ZFST / _ZIST = 1 the y inverse, y forward,
+    z forward and (one row per thread) z inverse passes write their output
+    tiles with tensor stores; with
     HYDFT_TMA=0 every thread loads its own elements.  Same fields to the
     bit, after steps and in the right-hand side."""
     kw = dict(ION, nx=128, ny=128, nz=128, lx=64.0, ly=64.0, lz=64.0, closure="maxwell", tau_model="constant",
               tau=1.5, dt=0.01, gpu_precision=prec)
+    names = ("HYDFT_TMA", "HYDFT_TMA_ZINV", "HYDFT_TMA_YST", "HYDFT_TMA_YFST", "HYDFT_TMA_ZFST", "HYDFT_TMA_ZIST",
+             "HYDFT_ZNB")
+    configs = [("0", "0", "0", "0", "0", "0", "2"),   # per-thread loads and stores
+               ("1", "1", "1", "1", "1", "0", "2"),   # tensor loads (z inverse too), tensor stores
+               ("1", "0", "1", "1", "1", "1", "1")]   # one row per thread in the z inverse, its tensor store
     out = []
-    for flag in ("0", "1"):
-        monkeypatch.setenv("HYDFT_TMA", flag)
-        monkeypatch.setenv("HYDFT_TMA_ZINV", flag)
+    for cfg in configs:
+        for name, val in zip(names, cfg):
+            monkeypatch.setenv(name, val)
         m = hg.Model(hg.default_params(**kw))
         n, mom, pi = seeded_state(m, seed=9)
         m.set_state(n, mom, pi)
@@ -385,11 +393,12 @@ def test_tma_tile_loads_give_identical_results(hg, monkeypatch, prec):
         m.advance(3)
         out.append(list(m.get_state()) + list(r))
         m.close()
-    monkeypatch.delenv("HYDFT_TMA")
-    monkeypatch.delenv("HYDFT_TMA_ZINV")
-    for x, y in zip(out[0], out[1]):
+    for name in names:
+        monkeypatch.delenv(name)
+    for x, y, z in zip(out[0], out[1], out[2]):
         if x is not None:
             assert np.array_equal(x, y)
+            assert np.array_equal(x, z)
 
 
 @pytest.mark.parametrize("prec", ["fp32", "fp64"])
@@ -445,9 +454,10 @@ def test_wide_yz_blocks_give_identical_results(hg, monkeypatch, prec, base):
 @pytest.mark.parametrize("prec", ["fp32", "fp64"])
 def test_z_pass_row_pairs_give_identical_results(hg, monkeypatch, prec):
     """The z passes can transform two ky rows per thread (both columns loaded
-    before the first is transformed; the inverse pass does by default, the
-    forward one with HYDFT_ZNB_FWD=2); the fields equal those of one row per
-    thread in both passes to the bit."""
+    before the first is transformed; the inverse pass does in the ensemble
+    forms, and both with HYDFT_ZNB=2 / HYDFT_ZNB_FWD=2); the fields equal
+    those of one row per thread in both passes (the inverse one then writing
+    its output tiles with tensor stores) to the bit."""
     kw = dict(ION, nx=64, ny=32, nz=48, lx=32.0, ly=16.0, lz=24.0, closure="maxwell", tau_model="constant",
               tau=1.5, dt=0.01, gpu_precision=prec)
     out = []
