@@ -331,6 +331,8 @@ int hydft_gpu_get_scalar(const hydft_gpu *h, const char *name, double *v)
         const int i = k == "yz_tile" ? 0 : k == "yz_threads" ? 1 : k == "yz_tile_fwd" ? 2 : k == "yz_threads_fwd" ? 3 : 4;
         *v = t[i];
     }
+    else if (k == "radix_x" || k == "radix_y" || k == "radix_z")
+        *v = h->s->radix_code(k == "radix_x" ? 0 : (k == "radix_y" ? 1 : 2));
     else if (k == "band_axes") *v = h->s->band_axes();
     else if (k == "ext_omega") *v = m.ext_omega;
     else if (k == "hnc_niter") *v = m.hnc_niter;

@@ -103,6 +103,9 @@ public:
     // tile shapes in use: kx columns and threads per y/z block of the
     // inverse passes, the same of the forward passes, threads per x block
     virtual void tiles(int *t5) const = 0;
+    // radix plan of axis 0/1/2 as decimal digits (843: radix 8, 4, 3),
+    // negative when the autotuner did not choose it
+    virtual int radix_code(int axis) const = 0;
     // axes whose passes classify band elements at compile time (x 1, y 2, z 4)
     virtual int band_axes() const = 0;
     // Records the launches of one RK3 step (after tuning) without running

@@ -1611,6 +1611,13 @@ public:
 
     int prepare() override { return tune(); }
 
+    int radix_code(int axis) const override
+    {
+        const FFTPlan &p = axis == 0 ? g.px : (axis == 1 ? g.py : g.pz);
+        int c = 0;
+        for (int i = 0; i < p.nrad; ++i) c = 10 * c + p.rad[i];
+        return radix_tuned ? c : -c;
+    }
     void tiles(int *t) const override
     {
         t[0] = yz_tx;
@@ -1739,13 +1746,18 @@ public:
 
     size_t device_bytes() const override { return alloc_bytes; }
 
-    // Autotuner of the tile shapes: times the phase-B transform sequence
-    // (y/z inverse of its inputs, x pass B, y/z forward of its outputs) with
-    // each candidate shape on the current data, writing only work buffers,
-    // and keeps for each of the three groups the shape that ran it fastest.  Every shape gives the same results to the bit
-    // (the same arithmetic per element, only the blocking differs).  The
-    // choice is shared by every model of the same grid, precision and
-    // physics in the process.  HYDFT_TUNE=0 keeps the defaults.
+    // Autotuner of the tile shapes and radix plans: times the phase-B
+    // transform sequence (y/z inverse of its inputs, x pass B, y/z forward of
+    // its outputs) with each candidate on the current data, writing only work
+    // buffers.  Tile shapes (register-plan axes): it keeps for each of the
+    // three groups the shape that ran it fastest; every shape gives the same
+    // results to the bit (the same arithmetic per element, only the blocking
+    // differs).  Radix plans (axes without a register plan, the generic
+    // Stockham passes): it keeps the sequence whose whole phase-B time was
+    // lowest; plans round differently, each within the oracle's tolerances.
+    // The choice is shared by every model of the same grid, precision and
+    // physics in the process.  HYDFT_TUNE=0 keeps the defaults, HYDFT_RADIX=0
+    // the set-up radix plans.
     struct TuneKey {
         int nx, ny, nz, bytes, nm, evolve, ext;
         bool operator<(const TuneKey &o) const
@@ -1754,12 +1766,59 @@ public:
         }
     };
     // cached shape: kx columns and threads per y/z block of the inverse and
-    // of the forward passes, threads per x block
-    static std::map<TuneKey, std::array<int, 5>> &tune_cache()
+    // of the forward passes, threads per x block; and the radix plans of the
+    // three axes
+    struct TuneVal {
+        std::array<int, 5> shape;
+        FFTPlan px, py, pz;
+    };
+    static std::map<TuneKey, TuneVal> &tune_cache()
     {
-        static std::map<TuneKey, std::array<int, 5>> m;
+        static std::map<TuneKey, TuneVal> m;
         return m;
     }
+
+    // Radix plans the autotuner tries for an axis of length L = 2^a 3^b that
+    // has no register plan (the generic Stockham passes): the 2^a part in
+    // radix-8 steps or in radix-4 steps (a last 4 or 2 for the remainder),
+    // the largest or the smallest radix first, the radix-3 steps after or
+    // before them.  Every plan is the same transform; only the pass sequence
+    // (and so the rounding) differs.
+    static std::vector<FFTPlan> radix_candidates(int L)
+    {
+        std::vector<FFTPlan> out;
+        int a = 0, b = 0, m = L;
+        while (m % 2 == 0) { m /= 2; ++a; }
+        while (m % 3 == 0) { m /= 3; ++b; }
+        if (m != 1 || L < 2 || L > MAX_L) return out;
+        for (int big : {8, 4}) {
+            std::vector<int> twos;
+            int r = a;
+            const int lb = big == 8 ? 3 : 2;
+            while (r >= lb) { twos.push_back(big); r -= lb; }
+            if (r == 2) twos.push_back(4);
+            else if (r == 1) twos.push_back(2);
+            for (int asc = 0; asc < 2; ++asc)
+                for (int threes_first = 0; threes_first < 2; ++threes_first) {
+                    std::vector<int> t2 = twos, seq;
+                    if (asc) std::sort(t2.begin(), t2.end());
+                    else std::sort(t2.rbegin(), t2.rend());
+                    const std::vector<int> t3(b, 3);
+                    if (threes_first) { seq = t3; seq.insert(seq.end(), t2.begin(), t2.end()); }
+                    else { seq = t2; seq.insert(seq.end(), t3.begin(), t3.end()); }
+                    if (seq.empty() || (int)seq.size() > MAX_RAD) continue;
+                    FFTPlan p{};
+                    p.L = L;
+                    p.nrad = (int)seq.size();
+                    for (size_t i = 0; i < seq.size(); ++i) p.rad[i] = seq[i];
+                    bool dup = false;
+                    for (const FFTPlan &q : out) dup = dup || (q.nrad == p.nrad && std::equal(q.rad, q.rad + q.nrad, p.rad));
+                    if (!dup) out.push_back(p);
+                }
+        }
+        return out;
+    }
+    bool radix_tuned = false;
     static std::mutex &tune_mutex()
     {
         static std::mutex m;
@@ -1793,17 +1852,30 @@ public:
             if (fx && (std::string(fx) == "128" || std::string(fx) == "256")) x_ntmax = std::atoi(fx);
             return 0;
         }
-        if (!(has_plan(g.ny) || has_plan(g.nz))) return 0;
+        // the radix plans of axes without a register plan are tuned too
+        // (HYDFT_RADIX=0 keeps the set-up plans)
+        const char *er = std::getenv("HYDFT_RADIX");
+        const bool radix_on = !(er && std::string(er) == "0");
+        auto generic = [](int L) { return L > 1 && !has_plan(L); };
+        const bool tile_tune = has_plan(g.ny) || has_plan(g.nz);
+        const bool radix_tune = radix_on && (generic(g.nx) || generic(g.ny) || generic(g.nz));
+        if (!tile_tune && !radix_tune) return 0;
         const TuneKey key{g.nx, g.ny, g.nz, (int)sizeof(R), nm, ph.evolve, ph.ext_active ? ph.ext_kind : 0};
         {
             std::lock_guard<std::mutex> lk(tune_mutex());
             auto it = tune_cache().find(key);
             if (it != tune_cache().end()) {
-                yz_tx = it->second[0];
-                yz_nt = it->second[1];
-                yz_txf = it->second[2];
-                yz_ntf = it->second[3];
-                x_ntmax = it->second[4];
+                yz_tx = it->second.shape[0];
+                yz_nt = it->second.shape[1];
+                yz_txf = it->second.shape[2];
+                yz_ntf = it->second.shape[3];
+                x_ntmax = it->second.shape[4];
+                if (radix_tune) {
+                    g.px = it->second.px;
+                    g.py = it->second.py;
+                    g.pz = it->second.pz;
+                    radix_tuned = true;
+                }
                 return 0;
             }
         }
@@ -1858,17 +1930,44 @@ public:
         const bool wide = g.ny == 256 || g.nz == 256;
         float bi = 1e30f, bx = 1e30f, bf = 1e30f;
         int btx = yz_tx, bynt = yz_nt, btxf = yz_txf, byntf = yz_ntf, bnt = x_ntmax;
-        for (int tx : txs)
-            for (int ynt : ynts)
-                for (int nt : nts) {
-                    if (!fast_x && nt != 256) continue;
-                    if (!wide && ynt != YZ_NT) continue;
-                    float ms[3];
-                    time_it(tx, ynt, nt, ms);
-                    if (ms[0] < bi) { bi = ms[0]; btx = tx; bynt = ynt; }
-                    if (ms[1] < bx) { bx = ms[1]; bnt = nt; }
-                    if (ms[2] < bf) { bf = ms[2]; btxf = tx; byntf = ynt; }
-                }
+        if (tile_tune)
+            for (int tx : txs)
+                for (int ynt : ynts)
+                    for (int nt : nts) {
+                        if (!fast_x && nt != 256) continue;
+                        if (!wide && ynt != YZ_NT) continue;
+                        float ms[3];
+                        time_it(tx, ynt, nt, ms);
+                        if (ms[0] < bi) { bi = ms[0]; btx = tx; bynt = ynt; }
+                        if (ms[1] < bx) { bx = ms[1]; bnt = nt; }
+                        if (ms[2] < bf) { bf = ms[2]; btxf = tx; byntf = ynt; }
+                    }
+        // radix plans: candidate i on every generic axis (an axis with fewer
+        // candidates keeps its last), timed over the whole phase-B sequence
+        // with the chosen tile shapes
+        if (radix_tune) {
+            const std::vector<FFTPlan> cx = generic(g.nx) ? radix_candidates(g.nx) : std::vector<FFTPlan>{g.px};
+            const std::vector<FFTPlan> cy = generic(g.ny) ? radix_candidates(g.ny) : std::vector<FFTPlan>{g.py};
+            const std::vector<FFTPlan> cz = generic(g.nz) ? radix_candidates(g.nz) : std::vector<FFTPlan>{g.pz};
+            const size_t nc = std::max(cx.size(), std::max(cy.size(), cz.size()));
+            FFTPlan best[3] = {g.px, g.py, g.pz};
+            float bt = 1e30f;
+            for (size_t i = 0; i < nc && !cx.empty() && !cy.empty() && !cz.empty(); ++i) {
+                g.px = cx[std::min(i, cx.size() - 1)];
+                g.py = cy[std::min(i, cy.size() - 1)];
+                g.pz = cz[std::min(i, cz.size() - 1)];
+                float ms[3];
+                time_it(btx, bynt, bnt, ms);
+                yz_txf = btxf;
+                yz_ntf = byntf;
+                const float tot = ms[0] + ms[1] + ms[2];
+                if (tot < bt) { bt = tot; best[0] = g.px; best[1] = g.py; best[2] = g.pz; }
+            }
+            g.px = best[0];
+            g.py = best[1];
+            g.pz = best[2];
+            radix_tuned = true;
+        }
         for (auto &e : tev) cudaEventDestroy(e);
         launches = launches0;
         yz_tx = btx;
@@ -1878,7 +1977,7 @@ public:
         x_ntmax = bnt;
         CK(cudaGetLastError());
         std::lock_guard<std::mutex> lk(tune_mutex());
-        tune_cache()[key] = {btx, bynt, btxf, byntf, bnt};
+        tune_cache()[key] = TuneVal{{btx, bynt, btxf, byntf, bnt}, g.px, g.py, g.pz};
         return 0;
     }
 

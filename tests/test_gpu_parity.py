@@ -472,3 +472,32 @@ def test_z_pass_row_pairs_give_identical_results(hg, monkeypatch, prec):
         m.close()
     for x, y in zip(out[0], out[1]):
         assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", TOL64), ("fp32", TOL32)])
+def test_tuned_radix_plans_match_oracle(hg, orc, monkeypatch, prec, tol):
+    """Axes without a register plan (72, 36, 24 here) run the generic
+    Stockham passes, whose radix sequence the autotuner picks: it times the
+    phase-B transforms with the 2^a part in radix-8 or radix-4 steps, either
+    order, the radix-3 steps first or last, and keeps the fastest (the
+    scalars radix_x/y/z give the chosen sequence as digits, positive when
+    the tuner chose it).  Whichever it keeps, five Maxwell steps match the
+    oracle."""
+    monkeypatch.delenv("HYDFT_RADIX", raising=False)
+    kw = dict(ION, nx=72, ny=36, nz=24, lx=36.0, ly=18.0, lz=12.0, closure="maxwell", tau_model="constant",
+              tau=1.5, dt=0.02, gpu_precision=prec)
+    m, o = pair(hg, orc, **kw)
+    n, mom, pi = seeded_state(m)
+    m.set_state(n, mom, pi)
+    n2, mom2, pi2 = m.get_state()
+    o.set_state(n2, mom2, pi2)
+    m.advance(5)
+    o.advance(5)
+    for ax, L in (("radix_x", 72), ("radix_y", 36), ("radix_z", 24)):
+        code = int(m.scalar(ax))
+        assert code > 0
+        assert int(np.prod([int(d) for d in str(code)])) == L
+    g = m.get_state()
+    assert rel(g[0], o.n) < tol, rel(g[0], o.n)
+    assert rel(g[1], o.mom) < tol, rel(g[1], o.mom)
+    assert rel(g[2], o.pi) < tol, rel(g[2], o.pi)
