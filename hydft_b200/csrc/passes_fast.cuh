@@ -547,6 +547,25 @@ __global__ void __launch_bounds__(TX * T * G) zfwd_tma_st(const __grid_constant_
     zfwd_body<R, T, E, TX, G, BAND, 1>(bk, g, a, twz, norm, tile, &om.m[bk.z]);
 }
 
+// The inverse z pass (one row per thread) with a tensor load of its input
+// tile into the exchange space (every column is read into registers before
+// the first exchange) and a tensor store of its output tile
+template <typename R, int T, int E, int TX, int G, bool BAND>
+__global__ void __launch_bounds__(TX * T * G) zinv_tma_st(const __grid_constant__ Grid g,
+    const __grid_constant__ PassArgs<R> a, const cplx<R> *twz, const __grid_constant__ TmaMaps tm,
+    const __grid_constant__ CUtensorMap otm, const __grid_constant__ TmaFields tf)
+{
+    const BlockIx bk = hw_block();
+    bool ok;
+    const cplx<R> *tile = tma_tile_begin<R, T * E>(&tm.m[bk.z], 2 * TX * (int)bk.x, G * (int)bk.y, 0, 0,
+                                                   (unsigned)(2 * TX * G * g.nkzc * sizeof(R)), ok);
+    if (!ok) {
+        if (threadIdx.x == 0) atomicOr(tf.status, ST_TIMEOUT);
+        return;
+    }
+    zinv_body<R, T, E, TX, G, BAND, 1>(bk, g, a, twz, tile, &otm, tf.dst[bk.z]);
+}
+
 // The inverse z pass (one row per thread) with a tensor store of its output
 // tile (map otm over the ZI buffer, field coordinate dst[f])
 template <typename R, int T, int E, int TX, int G, bool BAND>
@@ -565,10 +584,12 @@ template <typename R, int T, int E, int TX, int G, bool BAND>
 struct YinvTmaPack {
     static constexpr int MAXT = TX * T * G, MINB = 1;
     CUtensorMap tm;
+    CUtensorMap otm;   // the output tile's tensor store when store != 0
     Grid g;
     PassArgs<R> a;
     const cplx<R> *tw;
     TmaFields tf;
+    int store;
     __device__ __forceinline__ void run(const BlockIx &bk) const
     {
         bool ok;
@@ -578,7 +599,7 @@ struct YinvTmaPack {
             if (threadIdx.x == 0) atomicOr(tf.status, ST_TIMEOUT);
             return;
         }
-        yinv_body<R, T, E, TX, G, BAND>(bk, g, a, tw, tile);
+        yinv_body<R, T, E, TX, G, BAND>(bk, g, a, tw, tile, store ? &otm : nullptr, tf.dst[bk.z]);
     }
 };
 
@@ -586,10 +607,12 @@ template <typename R, int T, int E, int TX, int G, bool BAND>
 struct YfwdTmaPack {
     static constexpr int MAXT = TX * T * G, MINB = 1;
     CUtensorMap tm;
+    CUtensorMap otm;   // the output tile's tensor store when store != 0
     Grid g;
     PassArgs<R> a;
     const cplx<R> *tw;
     TmaFields tf;
+    int store;
     __device__ __forceinline__ void run(const BlockIx &bk) const
     {
         bool ok;
@@ -599,7 +622,7 @@ struct YfwdTmaPack {
             if (threadIdx.x == 0) atomicOr(tf.status, ST_TIMEOUT);
             return;
         }
-        yfwd_body<R, T, E, TX, G, BAND>(bk, g, a, tw, tile);
+        yfwd_body<R, T, E, TX, G, BAND>(bk, g, a, tw, tile, store ? &otm : nullptr, tf.dst[bk.z]);
     }
 };
 

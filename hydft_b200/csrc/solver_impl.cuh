@@ -482,10 +482,11 @@ public:
     // thread loads its own elements, as the ensemble forms always do; the
     // fields are the same to the bit either way)
     bool use_tma = true;
-    // the z inverse pass's TMA form (HYDFT_TMA_ZINV=1): its tile does not fit
-    // in the exchange buffer, and the extra shared memory costs blocks per SM
-    // (256^3 step 6.17 against 6.06 ms without it), so it is off by default
-    bool tma_zinv = false;
+    // the z inverse pass's tensor load (HYDFT_TMA_ZINV=0 switches it off):
+    // with one row per thread its tile goes into the exchange space; with two
+    // (HYDFT_ZNB=2) it does not fit there, and the extra shared memory cost
+    // blocks per SM (256^3 step 6.17 against 6.06 ms without the load)
+    bool tma_zinv = true;
     // tensor stores of the output tiles on the plain path: y inverse, y
     // forward, z forward, z inverse with one row per thread
     // (HYDFT_TMA_YST / _YFST / _ZFST / _ZIST = 0 switch them off)
@@ -794,7 +795,7 @@ public:
             const char *et = std::getenv("HYDFT_TMA");
             if (et && std::string(et) == "0") use_tma = false;
             const char *ez = std::getenv("HYDFT_TMA_ZINV");
-            if (ez) tma_zinv = std::string(ez) == "1";
+            if (ez && *ez) tma_zinv = std::string(ez) == "1";
             auto flag = [](const char *name, bool &v) {
                 const char *e = std::getenv(name);
                 if (e && *e) v = std::string(e) == "1";
@@ -931,7 +932,7 @@ public:
             constexpr int TX = decltype(TXc)::value;
             constexpr int G = yz_rows<T, TX, decltype(NTc)::value>();
             const size_t sm = yz_fast_smem<R>(T * E, T, TX, G);
-            auto go = [&](auto k, auto pk, auto kt, auto kst, int nb) {
+            auto go = [&](auto k, auto pk, auto kt, auto kst, auto kl, int nb) {
                 set_smem(k, sm);
                 const dim3 grid((g.nkxc + TX - 1) / TX, (g.nkyc + G * nb - 1) / (G * nb), nzf);
                 pk.g = g; pk.a = a; pk.tw = tpz;
@@ -942,6 +943,18 @@ public:
                     make_field_tmap<R>(&otm, zi, g.pkx, g.nkyc, g.nz, nin_max, TX, G, g.nz)) {
                     TmaFields tf = tma_fields(a.in, 0, zi, zsize);
                     for (int f = 0; f < nzf; ++f) tf.dst[f] = (int)((a.out[f] - zi) / (ptrdiff_t)zsize);
+                    // with HYDFT_TMA_ZINV=1 the input tile by a tensor load into
+                    // the exchange space as well
+                    const size_t tl = sizeof(cplx<R>) * (size_t)TX * G * g.nkzc;
+                    bool ld = tma_zinv && nzf <= 16 && tl + 8 <= sm - sizeof(cplx<R>) * 2 * T * E;
+                    TmaMaps maps;
+                    for (int f = 0; ld && f < nzf; ++f)
+                        ld = make_field_tmap<R>(&maps.m[f], a.in[f], g.pkx, g.nkyc, g.nkzc, 1, TX, G, g.nkzc);
+                    if (ld) {
+                        set_smem(kl, sm);
+                        launch("zinv", zbytes, [&] { kl<<<grid, TX * T * G, sm, st>>>(g, a, tpz, maps, otm, tf); });
+                        return;
+                    }
                     set_smem(kst, sm);
                     launch("zinv", zbytes, [&] { kst<<<grid, TX * T * G, sm, st>>>(g, a, tpz, otm, tf); });
                     return;
@@ -968,11 +981,11 @@ public:
                 launch_p("zinv", zbytes, grid, TX * T * G, sm, pk, [&] { k<<<grid, TX * T * G, sm, st>>>(g, a, tpz); });
             };
             if ((rec ? z_nb_ens : z_nb) == 2) {
-                if (band_z) go(zinv_fast<R, T, E, TX, G, true, 2>, ZinvPack<R, T, E, TX, G, true, 2>{}, zinv_tma<R, T, E, TX, G, true, 2>, zinv_st<R, T, E, TX, G, true>, 2);
-                else go(zinv_fast<R, T, E, TX, G, false, 2>, ZinvPack<R, T, E, TX, G, false, 2>{}, zinv_tma<R, T, E, TX, G, false, 2>, zinv_st<R, T, E, TX, G, false>, 2);
+                if (band_z) go(zinv_fast<R, T, E, TX, G, true, 2>, ZinvPack<R, T, E, TX, G, true, 2>{}, zinv_tma<R, T, E, TX, G, true, 2>, zinv_st<R, T, E, TX, G, true>, zinv_tma_st<R, T, E, TX, G, true>, 2);
+                else go(zinv_fast<R, T, E, TX, G, false, 2>, ZinvPack<R, T, E, TX, G, false, 2>{}, zinv_tma<R, T, E, TX, G, false, 2>, zinv_st<R, T, E, TX, G, false>, zinv_tma_st<R, T, E, TX, G, false>, 2);
             } else {
-                if (band_z) go(zinv_fast<R, T, E, TX, G, true, 1>, ZinvPack<R, T, E, TX, G, true, 1>{}, zinv_tma<R, T, E, TX, G, true, 1>, zinv_st<R, T, E, TX, G, true>, 1);
-                else go(zinv_fast<R, T, E, TX, G, false, 1>, ZinvPack<R, T, E, TX, G, false, 1>{}, zinv_tma<R, T, E, TX, G, false, 1>, zinv_st<R, T, E, TX, G, false>, 1);
+                if (band_z) go(zinv_fast<R, T, E, TX, G, true, 1>, ZinvPack<R, T, E, TX, G, true, 1>{}, zinv_tma<R, T, E, TX, G, true, 1>, zinv_st<R, T, E, TX, G, true>, zinv_tma_st<R, T, E, TX, G, true>, 1);
+                else go(zinv_fast<R, T, E, TX, G, false, 1>, ZinvPack<R, T, E, TX, G, false, 1>{}, zinv_tma<R, T, E, TX, G, false, 1>, zinv_st<R, T, E, TX, G, false>, zinv_tma_st<R, T, E, TX, G, false>, 1);
             }
             });
         });
@@ -1005,12 +1018,15 @@ public:
                     if (use_tma && tile + 8 <= sm - sizeof(cplx<R>) * 2 * T * E &&
                         make_field_tmap<R>(&pkt.tm, zi, g.pkx, g.nkyc, g.nz, nin_max, TX, g.nkyc, G)) {
                         pkt.g = g; pkt.a = b; pkt.tw = tpy; pkt.tf = tma_fields(b.in, nf, zi, zsize);
-                        // the output tile by a tensor store as well (HYDFT_TMA_YST=1)
-                        CUtensorMap otm;
-                        if (!rec && tma_yst && make_field_tmap<R>(&otm, yi, g.pkx, g.ny, g.nz, nin_max, TX, g.ny, G)) {
+                        // the output tile by a tensor store as well (plain and ensemble forms)
+                        pkt.store = 0;
+                        std::memset(static_cast<void *>(&pkt.otm), 0, sizeof(pkt.otm));
+                        if (tma_yst && make_field_tmap<R>(&pkt.otm, yi, g.pkx, g.ny, g.nz, nin_max, TX, g.ny, G)) {
                             for (int f = 0; f < nf; ++f) pkt.tf.dst[f] = (int)((b.out[f] - yi) / (ptrdiff_t)ysize);
+                            pkt.store = 1;
                             set_smem(kst, sm);
-                            launch("yinv", ybytes, [&] { kst<<<grid, TX * T * G, sm, st>>>(g, b, tpy, pkt.tm, otm, pkt.tf); });
+                            launch_p("yinv", ybytes, grid, TX * T * G, sm, pkt,
+                                     [&] { kst<<<grid, TX * T * G, sm, st>>>(g, b, tpy, pkt.tm, pkt.otm, pkt.tf); });
                             return;
                         }
                         set_smem(kt, sm);
@@ -1061,11 +1077,14 @@ public:
                         make_field_tmap<R>(&pkt.tm, xo, g.pkx, g.ny, g.nz, nout_max, TX, g.ny, G)) {
                         pkt.g = g; pkt.a = b; pkt.tw = tpy; pkt.tf = tma_fields(b.in, nf, xo, ysize);
                         // the output tile [G][nkyc][TX] by a tensor store as well
-                        CUtensorMap otm;
-                        if (!rec && tma_yfst && make_field_tmap<R>(&otm, zi, g.pkx, g.nkyc, g.nz, nin_max, TX, g.nkyc, G)) {
+                        pkt.store = 0;
+                        std::memset(static_cast<void *>(&pkt.otm), 0, sizeof(pkt.otm));
+                        if (tma_yfst && make_field_tmap<R>(&pkt.otm, zi, g.pkx, g.nkyc, g.nz, nin_max, TX, g.nkyc, G)) {
                             for (int f = 0; f < nf; ++f) pkt.tf.dst[f] = (int)((b.out[f] - zi) / (ptrdiff_t)zsize);
+                            pkt.store = 1;
                             set_smem(kst, sm);
-                            launch("yfwd", ybytes, [&] { kst<<<grid, TX * T * G, sm, st>>>(g, b, tpy, pkt.tm, otm, pkt.tf); });
+                            launch_p("yfwd", ybytes, grid, TX * T * G, sm, pkt,
+                                     [&] { kst<<<grid, TX * T * G, sm, st>>>(g, b, tpy, pkt.tm, pkt.otm, pkt.tf); });
                             return;
                         }
                         set_smem(kt, sm);

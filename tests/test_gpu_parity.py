@@ -381,7 +381,8 @@ def test_tma_tile_loads_give_identical_results(hg, monkeypatch, prec):
              "HYDFT_ZNB")
     configs = [("0", "0", "0", "0", "0", "0", "2"),   # per-thread loads and stores
                ("1", "1", "1", "1", "1", "0", "2"),   # tensor loads (z inverse too), tensor stores
-               ("1", "0", "1", "1", "1", "1", "1")]   # one row per thread in the z inverse, its tensor store
+               ("1", "0", "1", "1", "1", "1", "1"),   # one row per thread in the z inverse, its tensor store
+               ("1", "1", "1", "1", "1", "1", "1")]   # ... and its tensor load
     out = []
     for cfg in configs:
         for name, val in zip(names, cfg):
@@ -395,10 +396,10 @@ def test_tma_tile_loads_give_identical_results(hg, monkeypatch, prec):
         m.close()
     for name in names:
         monkeypatch.delenv(name)
-    for x, y, z in zip(out[0], out[1], out[2]):
-        if x is not None:
-            assert np.array_equal(x, y)
-            assert np.array_equal(x, z)
+    for fields in zip(*out):
+        if fields[0] is not None:
+            for other in fields[1:]:
+                assert np.array_equal(fields[0], other)
 
 
 @pytest.mark.parametrize("prec", ["fp32", "fp64"])
