@@ -1186,27 +1186,47 @@ __device__ __forceinline__ void xa_regs_body(const BlockIx &bk, const Grid &g, c
         p0[r].x = inv_mn;
     }
     if (!UONLY) {
+        // (m_1, m_2) wait in the warp's own staging space, whose inputs are
+        // consumed, while the output pairs are transformed: 2E fewer live
+        // registers per thread (the kernel spilled with them all in
+        // registers).  Lane l keeps element r at entry r 32 + l of the warp's
+        // four field slices (4 x 32/T rows x pkx entries >= 32 E, as
+        // pkx > L/3); the warp reads the same entries it wrote.
+        const int slice = RPW * pk;
+        auto stash = [&](int r) -> cplx<R> & {
+            const int e = r * 32 + lane;
+            return sb[((size_t)(e / slice) * rb + w * RPW) * pk + e % slice];
+        };
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < E; ++r) stash(r) = p1[r];
         // outputs: 0..2 u_d, 3..8 fluxes (00, 01, 02, 11, 12, 22), 9 mu
         x_r2c_pair<R, T, E, BAND, 1>(v, a.out[9], a.out[0], row, rowok, t, g, xrow, tw);
 #pragma unroll
-        for (int r = 0; r < E; ++r) v[r] = cplx<R>{p1[r].x * p0[r].x, p1[r].y * p0[r].x};
+        for (int r = 0; r < E; ++r) {
+            const cplx<R> q = stash(r);
+            v[r] = cplx<R>{q.x * p0[r].x, q.y * p0[r].x};
+        }
         x_r2c_pair<R, T, E, BAND, 1>(v, a.out[1], a.out[2], row, rowok, t, g, xrow, tw);
 #pragma unroll
         for (int r = 0; r < E; ++r) {
+            const cplx<R> q = stash(r);
             const R u0 = p0[r].y * p0[r].x;
-            v[r] = cplx<R>{p0[r].y * u0, p0[r].y * (p1[r].x * p0[r].x)};
+            v[r] = cplx<R>{p0[r].y * u0, p0[r].y * (q.x * p0[r].x)};
         }
         x_r2c_pair<R, T, E, BAND, 1>(v, a.out[3], a.out[4], row, rowok, t, g, xrow, tw);
 #pragma unroll
         for (int r = 0; r < E; ++r) {
-            const R u1 = p1[r].x * p0[r].x, u2 = p1[r].y * p0[r].x;
-            v[r] = cplx<R>{p0[r].y * u2, p1[r].x * u1};
+            const cplx<R> q = stash(r);
+            const R u1 = q.x * p0[r].x, u2 = q.y * p0[r].x;
+            v[r] = cplx<R>{p0[r].y * u2, q.x * u1};
         }
         x_r2c_pair<R, T, E, BAND, 1>(v, a.out[5], a.out[6], row, rowok, t, g, xrow, tw);
 #pragma unroll
         for (int r = 0; r < E; ++r) {
-            const R u2 = p1[r].y * p0[r].x;
-            v[r] = cplx<R>{p1[r].x * u2, p1[r].y * u2};
+            const cplx<R> q = stash(r);
+            const R u2 = q.y * p0[r].x;
+            v[r] = cplx<R>{q.x * u2, q.y * u2};
         }
         x_r2c_pair<R, T, E, BAND, 1>(v, a.out[7], a.out[8], row, rowok, t, g, xrow, tw);
     } else {
